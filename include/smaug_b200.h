@@ -1,0 +1,179 @@
+/*
+ * smaug_b200.h -- C ABI of the B200-native SMAUG time-advance engine.
+ *
+ * The engine replaces the single-GPU time-advance path of SMAUG (Sheffield
+ * MHD code, mikeg64/smaug): the host wrappers declared in the reference's
+ * include/smaugcukernels.h:8-93 and driven once per step by
+ * src/iosmaug.c:496-1144.  The reference calls ~40 wrappers per step, each
+ * launching 1-9 kernels with a host synchronisation after every launch; this
+ * library advances whole steps with a few fused kernels per step.
+ *
+ * Conventions (all unchanged from the reference):
+ *   - State layout: structure of arrays, field-major, x fastest:
+ *       w[f*n0*n1*n2 + (k*n1 + j)*n0 + i]            (src/gradops.cu:44-54)
+ *     field order 2D: rho mom1 mom2 energy b1 b2 energyb rhob b1b b2b
+ *                 3D: rho mom1 mom2 mom3 energy b1 b2 b3 energyb rhob b1b b2b b3b
+ *     (include/iotypes.h:209-216).  n[d] includes 2 ghost layers on each side.
+ *   - Positions: pos[d*n0*n1*n2 + cell] as read from the .ini file
+ *     (src/readwrite.c:1061-1068); the grid metric delx is derived from them
+ *     exactly as initgrid does (src/init.cu:2502-3060).
+ *   - Arithmetic: FP64 (the reference's real=double, include/iotypes.h:8-12).
+ *
+ * Every entry point returns 0 on success and a nonzero SMAUG_E* code on
+ * failure; smaug_last_error() returns a message for the calling thread's last
+ * failure.  A handle is owned by one host thread at a time; different handles
+ * are independent.
+ */
+#ifndef SMAUG_B200_H_
+#define SMAUG_B200_H_
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SMAUG_PARAMS_VERSION 1
+#define SMAUG_MAXVAR 13
+
+/* status codes */
+#define SMAUG_OK 0
+#define SMAUG_E_INVALID 1      /* bad argument or parameter block */
+#define SMAUG_E_CUDA 2         /* CUDA runtime error (message has the CUDA string) */
+#define SMAUG_E_NOMEM 3        /* device or host allocation failed */
+#define SMAUG_E_IO 4           /* file could not be read or written */
+#define SMAUG_E_FORMAT 5       /* malformed .ini/.out content */
+#define SMAUG_E_UNSUPPORTED 6  /* valid in the reference, not implemented here */
+#define SMAUG_E_NONFINITE 7    /* a NaN/Inf appeared in the evolved state */
+
+/* boundary types, numbering of p->boundtype (include/iotypes.h:139) */
+#define SMAUG_BC_PERIODIC 0
+#define SMAUG_BC_CONT 3
+#define SMAUG_BC_CONTCD4 4
+#define SMAUG_BC_FIXED 5
+#define SMAUG_BC_SYMM 6
+#define SMAUG_BC_ASYMM 7
+
+/* integrators */
+#define SMAUG_INT_EULER 0  /* the reference's rkon=0 single-stage step */
+#define SMAUG_INT_RK4 1    /* classical RK4 on the same spatial operator */
+
+/* precision forms */
+#define SMAUG_PREC_FP64 0
+
+/* fill model for the right-biased hyperdiffusion pad (see DESIGN) */
+#define SMAUG_PAD_STRAY 0  /* pad holds the stray tmp6 store, as observed */
+#define SMAUG_PAD_ZERO 1   /* pad holds zero */
+
+/* user source (driver) kinds */
+#define SMAUG_DRIVER_NONE 0
+#define SMAUG_DRIVER_GAUSS 1  /* m_0 += dt * v(x,t) * rho_t, v Gaussian in space */
+
+/*
+ * Run parameters.  Mirrors the fields of the reference's struct params
+ * (include/iotypes.h:85-175) that the time advance reads; the per-field
+ * boundtype[NVAR][NDIM][2] is given per dimension because the reference
+ * driver assigns the same type to every field (src/iosmaug.c:192-222).
+ */
+typedef struct smaug_params {
+  int32_t version;          /* SMAUG_PARAMS_VERSION */
+  int32_t ndim;             /* 2 or 3 */
+  int32_t n[3];             /* p->n: cells per dim including ghosts (n[2]=1 in 2D) */
+  int32_t moddton;          /* p->moddton: 1 = adaptive dt from the CFL max */
+  int32_t hyperdifmom;      /* p->hyperdifmom: 1 = hyperdiffusion on */
+  int32_t integrator;       /* SMAUG_INT_* */
+  int32_t precision;        /* SMAUG_PREC_* */
+  int32_t pad_model;        /* SMAUG_PAD_* */
+  int32_t boundtype[3][2];  /* p->boundtype[*][dim][0]=upper, [1]=lower */
+  int32_t driver;           /* SMAUG_DRIVER_* */
+  int32_t reserved_i[7];
+  double dx[3];             /* p->dx: (xmax-xmin)/(n-4), used by the dt rule */
+  double dt;                /* p->dt at start (the reference sets 1e-8 when moddton) */
+  double dtmax;             /* DT: adaptive dt is accepted only below this */
+  double courant;           /* p->courant */
+  double gamma;             /* p->gamma */
+  double eta;               /* p->eta (written to .out headers only) */
+  double g[3];              /* p->g: gravity */
+  double chyp[SMAUG_MAXVAR];/* p->chyp[field]: hyperdiffusion coefficients */
+  double xmin[3];           /* p->xmin (used by the .out writer metadata only) */
+  /* Gaussian driver: v = amp * sin(2 pi t / period) * prod_d exp(-((x_d-x0_d)/sigma_d)^2)
+     over dims with sigma_d > 0; period <= 0 means a steady driver. */
+  double drv_amp, drv_period;
+  double drv_x0[3];
+  double drv_sigma[3];
+  double reserved_d[8];
+} smaug_params_t;
+
+typedef struct smaug_engine* smaug_handle_t;
+
+/* Fill *p with the reference's Orszag-Tang defaults for an N0 x N1 interior
+   (models/iosmaugparams.h.ot): gamma 5/3, chyp 0.2, periodic, moddton. */
+int smaug_params_default(smaug_params_t* p, int32_t ndim);
+
+/*
+ * Create an engine on the current CUDA device.  Replaces cuinit
+ * (src/init.cu:2222-2448) + initgrid (src/init.cu:2502-3060) + the initial
+ * cuboundary sweep (src/iosmaug.c:480-488).
+ *   w   : NVAR*ncells doubles, reference layout (slot 0 as read from .ini)
+ *   pos : NDIM*ncells doubles, cell positions (wd[pos1..] of the reference)
+ */
+int smaug_create(const smaug_params_t* p, const double* w, const double* pos,
+                 smaug_handle_t* out);
+
+/* Advance nsteps steps.  Replaces the body of the step loop
+   src/iosmaug.c:496-1144 (cucomputedervfields ... cuboundary). */
+int smaug_step(smaug_handle_t h, int32_t nsteps);
+
+/* Copy the current state (all NVAR fields, ghosts included) to the host.
+   Replaces cuupdate (src/update.cu:165-233). */
+int smaug_get_state(smaug_handle_t h, double* w);
+
+/* Replace the evolved fields from a host array in reference layout. */
+int smaug_set_state(smaug_handle_t h, const double* w);
+
+/* Step counter, simulated time and the dt of the last step (state->it, t, dt). */
+int smaug_get_time(smaug_handle_t h, int64_t* it, double* t, double* dt);
+
+/* Per-dimension CFL maxima of the current state (p->cmax per dim,
+   src/computedervfields.cu:1864-2050). */
+int smaug_get_cmax(smaug_handle_t h, double* cmax);
+
+/* Write the current state as a reference .out file (src/readwrite.c:160-366).
+   `it` and `t` go to the header; name is the 79-byte run name. */
+int smaug_write_out(smaug_handle_t h, const char* path, const char* name,
+                    int32_t it, double t);
+
+/* Release all device memory of the handle. */
+int smaug_destroy(smaug_handle_t h);
+
+/* Message of the calling thread's last failure ("" if none). */
+const char* smaug_last_error(void);
+
+/* Library version string. */
+const char* smaug_version(void);
+
+/*
+ * Format boundary (host only, no device use).
+ * Read a reference ASCII .ini (src/readwrite.c:975-1082): header + one line
+ * per cell "pos[ndim] w[nvar]".  n[] must be set by the caller (the reference
+ * takes it from compile-time NI/NJ); the file's own n line is checked.
+ */
+int smaug_read_ini(const char* path, int32_t ndim, const int32_t* n,
+                   double* w, double* pos, int32_t* it, double* t);
+
+/* Write a reference binary .out (src/readwrite.c:160-366) from host arrays. */
+int smaug_write_out_host(const char* path, const smaug_params_t* p,
+                         const double* w, const double* pos, const char* name,
+                         int32_t it, double t);
+
+/* Grid metric from positions (host), the reference's initgrid
+   (src/init.cu:2502-3060): rewrites ghost positions by linear extrapolation
+   and fills delx[d*ncells + cell]. */
+int smaug_grid_metric(int32_t ndim, const int32_t* n, double* pos, double* delx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SMAUG_B200_H_ */

@@ -1,0 +1,153 @@
+"""Recipe: build the reference SMAUG GPU binary from its own sources.
+
+TEST INFRASTRUCTURE.  The reference (mikeg64/smaug) has no CPU solver: every
+solver routine is a CUDA kernel.  To pin the CPU oracle against the real
+reference, this script compiles the reference's unmodified solver sources for
+sm_100a and the result runs on the B200 box as a checker.  Nothing of the
+reference enters the repository: sources are copied to a scratch directory
+under /tmp, the build output goes to oracle/_ref/<name>/ (git-ignored).
+
+The reference's build selects a model by copying models/*.<model> over the
+compile-time parameter header and instantiates the shared device helpers by
+`sed s/MODID/<id>/` (src/Makefile:79-227); this recipe does the same for the
+Orszag-Tang model (`make ot`) with the run parameters substituted into
+include/iosmaugparams.h.  Three workarounds are needed with CUDA 12.9 / GCC 13:
+  1. src/init.cu:169 passes an undeclared `w`; it is built with `wmod`
+     (the only array in scope; the call is inside `if(p->readini==0)`,
+     not taken when an .ini is read).
+  2. the library list of src/Makefile:152 precedes the objects; linking is
+     done here with nvcc and the objects first.
+  3. most cu* wrappers return int but fall off the end without a return
+     (e.g. src/computedervfields.cu:1800-1830); GCC 13 compiles that to a
+     trap instruction at -O0 (nvcc's host pass), so host code is built with
+     -fno-unreachable-traps, which restores a plain return.
+Usage:  python oracle/build_ref.py NAME NI NJ NT [key=value ...]
+"""
+import glob
+import os
+import re
+import shutil
+import subprocess
+import sys
+import tempfile
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REFROOT = "/root/reference/smaug"
+OUT = os.path.join(HERE, "_ref")
+
+# sed instantiation table of src/Makefile:163-227: object -> [(template, id)]
+MODIDS = {
+    "nushk1.cu": [("gradops.cu", "nshk")],
+    "hyperdifvisc1.cu": [("gradops.cu", "hdv1")],
+    "hyperdifvisc1l.cu": [("gradops.cu", "hdv1l")],
+    "hyperdifvisc1r.cu": [("gradops.cu", "hdv1r")],
+    "hyperdifrhosource1.cu": [("gradops.cu", "hdr1")],
+    "hyperdifesource1.cu": [("gradops.cu", "hde1")],
+    "hyperdifbsource1.cu": [("gradops.cu", "hdb1")],
+    "hyperdifbsourcene1.cu": [("gradops.cu", "hdbne1")],
+    "hyperdifmomsource1.cu": [("gradops.cu", "hdm1")],
+    "hyperdifmomsourcene1.cu": [("gradops.cu", "hdmne1")],
+    "centdiff1.cu": [("gradops.cu", "cd1"), ("dervfields.cu", "cd1"), ("usersource.cu", "cd1")],
+    "centdiff2.cu": [("gradops.cu", "cd2"), ("dervfields.cu", "cd2"), ("usersource.cu", "cd2")],
+    "computedervfields.cu": [("gradops.cu", "cdf"), ("dervfields.cu", "cdf")],
+    "boundary.cu": [("gradops.cu", "b")],
+    "init.cu": [("gradops.cu", "i"), ("init_user.cu", "i")],
+    "update.cu": [("gradops.cu", "u")],
+    "advance.cu": [("gradops.cu", "adv"), ("dervfields.cu", "adv")],
+    "divb.cu": [("gradops.cu", "db"), ("dervfields.cu", "db")],
+}
+CFILES = ["iosmaug.c", "initialisation.c", "dxroutines.c", "readwrite.c"]
+
+DEFAULTS = {
+    "XMIN": "0.0", "XMAX": "6.283185307179586", "YMIN": "0.0", "YMAX": "6.283185307179586",
+    "DT": "1.0", "PCOURANT": "0.3", "PMODDTON": "1.0", "PCFGSAVEFREQUENCY": "1",
+    "PGAMMA": "1.66666667", "CHYP": "0.2", "CFGFILE": '"ref.ini"', "CFGOUT": '"out/ref"',
+}
+
+
+def _set_define(text, name, value):
+    pat = re.compile(r"^#define\s+%s\s+.*$" % name, re.M)
+    if not pat.search(text):
+        raise RuntimeError("define %s not found" % name)
+    return pat.sub("#define %s %s" % (name, value), text)
+
+
+def build_ref(name, ni, nj, nt, arch="sm_100a", verbose=True, **kw):
+    if not os.path.isdir(REFROOT):
+        raise RuntimeError("reference sources not present at %s" % REFROOT)
+    cfg = dict(DEFAULTS)
+    cfg.update({k.upper(): str(v) for k, v in kw.items()})
+    dest = os.path.join(OUT, name)
+    os.makedirs(dest, exist_ok=True)
+    tmp = tempfile.mkdtemp(prefix="smaug_ref_")
+    try:
+        for d in ("src", "include", "models"):
+            shutil.copytree(os.path.join(REFROOT, d), os.path.join(tmp, d))
+        subprocess.check_call(["chmod", "-R", "u+w", tmp])
+        src, inc, mod = (os.path.join(tmp, d) for d in ("src", "include", "models"))
+        # make ot (src/Makefile:98-101)
+        shutil.copy(os.path.join(mod, "iosmaugparams.h.ot"), os.path.join(inc, "iosmaugparams.h"))
+        shutil.copy(os.path.join(mod, "init_user.cu.ot"), os.path.join(src, "init_user.cu"))
+        shutil.copy(os.path.join(mod, "boundary.cu.ot"), os.path.join(src, "boundary.cu"))
+        ph = os.path.join(inc, "iosmaugparams.h")
+        text = open(ph).read()
+        text = _set_define(text, "NI", str(ni))
+        text = _set_define(text, "NJ", str(nj))
+        text = _set_define(text, "NT", str(nt))
+        for k in ("XMIN", "XMAX", "YMIN", "YMAX", "DT", "PCOURANT", "PMODDTON",
+                  "PCFGSAVEFREQUENCY", "PGAMMA", "CFGFILE", "CFGOUT"):
+            text = _set_define(text, k, cfg[k])
+        for k in ("PCHYP", "PCHYPRHO", "PCHYPENERGY", "PCHYPB0", "PCHYPB1", "PCHYPB2",
+                  "PCHYPMOM0", "PCHYPMOM1", "PCHYPMOM2"):
+            text = _set_define(text, k, cfg.get(k, cfg["CHYP"]))
+        open(ph, "w").write(text)
+        # workaround 1 (see module docstring)
+        initcu = os.path.join(src, "init.cu")
+        lines = open(initcu).read().split("\n")
+        if "init_user_i(w,p,ii)" not in lines[168]:
+            raise RuntimeError("unexpected src/init.cu:169: %r" % lines[168])
+        lines[168] = lines[168].replace("init_user_i(w,p,ii)", "init_user_i(wmod,p,ii)")
+        open(initcu, "w").write("\n".join(lines))
+        # MODID instantiation
+        for cu, pairs in MODIDS.items():
+            for tpl, mid in pairs:
+                t = open(os.path.join(src, tpl)).read().replace("MODID", mid)
+                base = tpl[:-3]
+                open(os.path.join(inc, "%s_%s.cuh" % (base, mid)), "w").write(t)
+        objs = []
+        for cu in MODIDS:
+            o = os.path.join(src, cu[:-3] + ".o")
+            cmd = ["nvcc", "-arch=" + arch, "-maxrregcount=32", "-DUSE_SAC", "-w",
+                   "-Xcompiler", "-fno-unreachable-traps",
+                   "-o", o, "-c", os.path.join(src, cu)]
+            if verbose:
+                print(" ".join(cmd), flush=True)
+            subprocess.check_call(cmd, cwd=src)
+            objs.append(o)
+        for c in CFILES:
+            o = os.path.join(src, c[:-2] + ".o")
+            cmd = ["g++", "-O0", "-fno-unreachable-traps", "-DUSE_SAC", "-DD1D", "-w", "-fpermissive",
+                   "-o", o, "-c", os.path.join(src, c)]
+            if verbose:
+                print(" ".join(cmd), flush=True)
+            subprocess.check_call(cmd, cwd=src)
+            objs.append(o)
+        binp = os.path.join(dest, "smaug")
+        cmd = ["nvcc", "-arch=" + arch, "-o", binp] + objs + ["-lcudart", "-lm"]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.check_call(cmd, cwd=src)
+        with open(os.path.join(dest, "build.txt"), "w") as f:
+            f.write("ni=%d nj=%d nt=%d %s\n" % (ni, nj, nt, cfg))
+        return binp
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+
+
+if __name__ == "__main__":
+    a = sys.argv[1:]
+    if len(a) < 4:
+        print(__doc__)
+        sys.exit(2)
+    kw = dict(x.split("=", 1) for x in a[4:])
+    print(build_ref(a[0], int(a[1]), int(a[2]), int(a[3]), **kw))

@@ -1,0 +1,1145 @@
+// engine.cu -- B200 (sm_100a) time-advance engine for SMAUG, FP64.
+//
+// One fused kernel per stage evaluates the whole spatial operator of the
+// reference's single-stage step (src/iosmaug.c:631-835) for a 2D tile:
+//   state tile + 3-cell halo staged in shared memory
+//   -> directional fluxes + 4th-order divergence     (src/centdiff1.cu, centdiff2.cu)
+//   -> background energy coupling, gravity            (src/centdiff2.cu:80-154)
+//   -> hyperdiffusion nu_r/nu_l and sources            (src/hyperdifvisc1{r,l}.cu,
+//                                                      src/hyperdif*source*.cu)
+//   -> user driver                                     (source_parallel)
+//   -> stage combine (Euler or classical RK4), ghost images (src/boundary.cu)
+//   -> per-dimension CFL maxima of the written state (src/computedervfields.cu:1864-2050)
+// The CFL maxima of a stage's input are produced by the previous launch's
+// epilogue, so no launch waits for the host: a step is 1 (Euler) or 4 (RK4)
+// launches and the dt rule (src/iosmaug.c:541-616) runs on the device.
+//
+// Arithmetic follows the reference's expression trees term by term (same
+// divisions, same accumulation order per cell) so that results agree with the
+// reference's FP64 output to rounding.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/smaug_b200.h"
+#include "engine_internal.h"
+
+#define SMAUG_VERSION_STRING "smaug_b200 0.1 (sm_100a, fp64)"
+
+namespace smaug {
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+static thread_local std::string g_err;
+
+int set_error(int code, const char* fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return code;
+}
+void clear_error() { g_err.clear(); }
+const char* last_error() { return g_err.c_str(); }
+
+#define CUDA_TRY(call)                                                            \
+  do {                                                                            \
+    cudaError_t _e = (call);                                                      \
+    if (_e != cudaSuccess)                                                        \
+      return smaug::set_error(SMAUG_E_CUDA, "%s failed: %s (%s:%d)", #call,       \
+                       cudaGetErrorString(_e), __FILE__, __LINE__);               \
+  } while (0)
+
+// ---------------------------------------------------------------------------
+// kernel parameters
+// ---------------------------------------------------------------------------
+constexpr int TX = 32;             // tile width (x, fastest)
+constexpr int TY = 8;              // tile height
+constexpr int HALO = 3;            // stencil radius of the hyperdiffusion windows
+constexpr int RX = TX + 2 * HALO;  // staged region
+constexpr int RY = TY + 2 * HALO;
+constexpr int RC = RX * RY;
+constexpr int NTHREADS = TX * TY;
+constexpr int NF2 = 10;            // 2D fields: 6 evolved + 4 background
+constexpr int NSCR = 7;            // scratch arrays of RC doubles
+constexpr size_t SMEM2D = sizeof(double) * (size_t)(NF2 + NSCR) * RC;
+
+// 2D field ids (include/iotypes.h:209-216)
+enum { RHO = 0, M1 = 1, M2 = 2, EN = 3, B1 = 4, B2 = 5, EB = 6, RHOB = 7, BB1 = 8, BB2 = 9 };
+
+struct KParams {
+  int n0, n1;
+  long ncell;
+  int bt[3];        // boundtype[dim][0] (upper) -- gradient edge zeroing
+  int bc[3];        // ghost-fill type per dim
+  double gamma, courant, dtmax;
+  double dx[3];
+  double g[3];
+  double chyp[SMAUG_MAXVAR];
+  int moddton, hyperdif, has_bg, has_grav, driver;
+  double drv_amp, drv_period, drv_x0[3], drv_sigma[3];
+};
+
+struct KBufs {
+  const double* uin;   // [6][ncell] stage input (ghosts valid)
+  const double* un;    // [6][ncell] RK base state
+  double* uout;        // [6][ncell] stage output
+  double* acc;         // [6][ncell] RK accumulator
+  const double* bg;    // [4][ncell] energyb, rhob, b1b, b2b
+  const double* delx[3];
+  const double* pos[3];
+  const int* padsrc[3];
+  const double* cmax_in;          // [3]
+  unsigned long long* cmax_out;   // [3] (double bits, atomicMax)
+  unsigned long long* cmax_clear; // [3] zeroed for the launch after next
+  const double* dt_prev;          // dt of the previous step
+  double* dt_new;                 // dt of this step (written by stage 0)
+  const double* t_prev;
+  double* t_new;
+  int* flags;
+  int mode;   // SMAUG_INT_EULER / SMAUG_INT_RK4
+  int stage;  // 0..3
+};
+
+// ---------------------------------------------------------------------------
+// device helpers
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double dmax0(double m, double v) { return (v > m) ? v : m; }
+
+// dt rule, src/iosmaug.c:541-616 (a rejected candidate keeps the previous dt,
+// see the oracle's dt_rule for why)
+__device__ double device_dt(const KParams& P, const double* cmax, double dt_prev, int nd) {
+  if (P.moddton != 1) return dt_prev;
+  double courantmax = 1.0e-12;
+  double cm = cmax[nd - 1];
+  for (int d = 0; d < nd; d++) {
+    double t = cm / P.dx[d];
+    if (t > courantmax) courantmax = t;
+  }
+  double dttemp = P.courant / courantmax;
+  if (dttemp > 1.0e-12 && dttemp < P.dtmax) return dttemp;
+  return dt_prev;
+}
+
+// computec3 (src/dervfields.cu:241-309), 2D, fast speed along `dir`
+__device__ __forceinline__ double cfast2(double gamma, double rho, double m1, double m2, double e,
+                                         double b1, double b2, double eb, double rhob, double bb1,
+                                         double bb2, int dir) {
+  double m2s = m1 * m1 + m2 * m2;
+  double b2s = b1 * b1 + b2 * b2;
+  double bbb = bb1 * b1 + bb2 * b2;
+  double bb2s = bb1 * bb1 + bb2 * bb2;
+  double rt = rho + rhob;
+  double pk = (gamma - 1) * (e - 0.5 * (m2s / rt) - 0.5 * b2s - bbb);
+  double cs2 = (gamma * (pk + (gamma - 1) * (eb - 0.5 * bb2s))) / rt;
+  double cf = (b2s + bb2s + 2.0 * bbb) / rt + cs2;
+  double bd = (dir == 0) ? (bb1 + b1) : (bb2 + b2);
+  double md = (dir == 0) ? m1 : m2;
+  double cfasti = 0.5 * (cf + sqrt(cf * cf - 4.0 * cs2 * (bd * bd) / rt));
+  return sqrt(cfasti) + fabs(md / rt);
+}
+
+// ghost images of interior index a along a dimension of n cells (the
+// reference's fill of ghost indices from interior sources, per type)
+__device__ __forceinline__ int ghost_images(int a, int n, int type, int* img) {
+  int c = 0;
+  switch (type) {
+    case SMAUG_BC_PERIODIC:
+      if (a == n - 4 || a == n - 3) img[c++] = a - (n - 4);
+      if (a == 2 || a == 3) img[c++] = a + n - 4;
+      break;
+    case SMAUG_BC_CONTCD4:
+      if (a == 4) img[c++] = 0;
+      if (a == 3) img[c++] = 1;
+      if (a == n - 4) img[c++] = n - 2;
+      if (a == n - 5) img[c++] = n - 1;
+      break;
+    case SMAUG_BC_CONT:
+      if (a == 2) { img[c++] = 0; img[c++] = 1; }
+      if (a == n - 3) { img[c++] = n - 2; img[c++] = n - 1; }
+      break;
+    case SMAUG_BC_SYMM:
+      if (a == 3) img[c++] = 0;
+      if (a == 2) img[c++] = 1;
+      if (a == n - 4) img[c++] = n - 1;
+      if (a == n - 3) img[c++] = n - 2;
+      break;
+    default:
+      break;
+  }
+  return c;
+}
+
+// edge zeroing of the gradient operators when boundtype != 0
+// (src/gradops.cu:459-474 for grad3dn, :620-823 for the 2nd-order ones;
+// evaluated for cells whose other coordinates are inside the band, where the
+// reference's precedence-dependent conditions reduce to these sets)
+__device__ __forceinline__ bool zero3dn(int a, int n) {
+  return a == 2 || a == 3 || a == n - 4 || a == n - 3;
+}
+__device__ __forceinline__ bool zero1n(int a, int n) {
+  return a == 1 || a == 2 || a == n - 3 || a == n - 2;
+}
+
+// ---------------------------------------------------------------------------
+// 2D stage kernel
+// ---------------------------------------------------------------------------
+struct Tile {
+  double* S;  // [NF2][RC]
+  double* X;  // [NSCR][RC]
+  int x0, y0;
+  __device__ __forceinline__ double& s(int f, int lx, int ly) const { return S[f * RC + ly * RX + lx]; }
+  __device__ __forceinline__ double& x(int k, int lx, int ly) const { return X[k * RC + ly * RX + lx]; }
+};
+
+// q of a hyperdiffusion pass (hyperdifvisc1r_parallel tmp6,
+// src/hyperdifvisc1r.cu:1225-1253) from the 10 field values
+__device__ __forceinline__ double hq2(int kind, int comp, const double* v) {
+  switch (kind) {
+    case 0:  // rho
+      return v[RHO];
+    case 1: {  // energy: e - (B'^2 + m^2/rho_t)/2
+      return v[EN] - 0.5 * ((v[B1] * v[B1] + v[B2] * v[B2]) +
+                            (v[M1] * v[M1] + v[M2] * v[M2]) / (v[RHO] + v[RHOB]));
+    }
+    case 2:  // velocity component
+      return v[M1 + comp] / ((v[RHO] + v[RHOB]));
+    default:  // magnetic perturbation component
+      return v[B1 + comp];
+  }
+}
+
+__device__ __forceinline__ double ptot2(double gamma, const double* v) {
+  // computept3 (src/dervfields.cu:107-153)
+  double pt = (gamma - 2.0) * ((v[B1] * v[BB1] + v[B2] * v[BB2]) + 0.5 * (v[B1] * v[B1] + v[B2] * v[B2]));
+  return (gamma - 1.0) * (v[EN] - 0.5 * (v[M1] * v[M1] + v[M2] * v[M2]) / (v[RHO] + v[RHOB])) - pt;
+}
+
+__device__ __forceinline__ void load_cell(const Tile& T, int lx, int ly, double* v) {
+#pragma unroll
+  for (int f = 0; f < NF2; f++) v[f] = T.s(f, lx, ly);
+}
+
+// fluxes along d of rho, m1, m2, e and the transverse B component
+// (src/centdiff1.cu:51-197, src/centdiff2.cu:203-323)
+__device__ __forceinline__ void fluxes2(double gamma, const double* v, int d, double* F) {
+  double rt = v[RHO] + v[RHOB];
+  double md = v[M1 + d];
+  double pt = ptot2(gamma, v);
+  // rho
+  F[0] = md * v[RHO] / rt + (v[RHOB] * md) / (v[RHOB] + v[RHO]);
+  // momentum components
+#pragma unroll
+  for (int c = 0; c < 2; c++) {
+    double bf = v[B1 + c], bbf = v[BB1 + c], bbd = v[BB1 + d], bd = v[B1 + d];
+    double fm = (d == c) ? pt - (bf * bbd + bbf * bd) - bf * bd : -(bf * bbd + bbf * bd) - bf * bd;
+    double x = 0.0;
+    x += md * v[M1 + c] / rt + fm;
+    F[1 + c] = x;
+  }
+  // energy
+  {
+    double bbm = v[BB1] * v[M1] + v[BB2] * v[M2];
+    double bm = v[B1] * v[M1] + v[B2] * v[M2];
+    double ft = md * (pt);
+    ft -= v[B1 + d] * bbm;
+    ft -= v[BB1 + d] * bm;
+    ft /= rt;
+    ft += md * v[EB] / rt;
+    ft -= v[B1 + d] * bm / rt;
+    F[3] = md * v[EN] / rt + ft;
+  }
+  // B component c != d
+  {
+    int c = 1 - d;
+    F[4] = md * v[B1 + c] / rt - (v[B1 + d] + v[BB1 + d]) * v[M1 + c] / rt +
+           (v[BB1 + c]) * v[M1 + d] / rt;
+  }
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(NTHREADS, 2) stage2d_kernel(const KParams P, const KBufs B) {
+  extern __shared__ double smem[];
+  Tile T;
+  T.S = smem;
+  T.X = smem + NF2 * RC;
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
+  T.x0 = 2 + blockIdx.x * TX;
+  T.y0 = 2 + blockIdx.y * TY;
+  const int n0 = P.n0, n1 = P.n1;
+  const long nc = P.ncell;
+
+  // ---- stage the state tile ------------------------------------------
+  for (int r = tid; r < RC; r += NTHREADS) {
+    int lx = r % RX, ly = r / RX;
+    int gi = T.x0 - HALO + lx, gj = T.y0 - HALO + ly;
+    bool in = gi >= 0 && gi < n0 && gj >= 0 && gj < n1;
+    long c = (long)gj * n0 + gi;
+#pragma unroll
+    for (int f = 0; f < 6; f++) T.S[f * RC + r] = in ? B.uin[f * nc + c] : 0.0;
+#pragma unroll
+    for (int f = 0; f < 4; f++) T.S[(6 + f) * RC + r] = in ? B.bg[f * nc + c] : (f == 1 ? 1.0 : 0.0);
+  }
+
+  // ---- dt of this step and stage time ----------------------------------
+  double dt, tstage;
+  if (B.stage == 0) {
+    dt = device_dt(P, B.cmax_in, *B.dt_prev, 2);
+    if (blockIdx.x == 0 && blockIdx.y == 0 && tid == 0) {
+      *B.dt_new = dt;
+      *B.t_new = *B.t_prev + dt;
+      B.cmax_clear[0] = B.cmax_clear[1] = B.cmax_clear[2] = 0ull;
+    }
+    tstage = *B.t_prev;
+  } else {
+    dt = *B.dt_new;
+    tstage = *B.t_prev + (B.stage == 3 ? dt : 0.5 * dt);
+    if (blockIdx.x == 0 && blockIdx.y == 0 && tid == 0)
+      B.cmax_clear[0] = B.cmax_clear[1] = B.cmax_clear[2] = 0ull;
+  }
+  __syncthreads();
+
+  const int lxo = tx + HALO, lyo = ty + HALO;
+  const int gi = T.x0 + tx, gj = T.y0 + ty;
+  const bool active = gi <= n0 - 3 && gj <= n1 - 3;
+  const int gidx[2] = {gi, gj};
+  const int nn[2] = {n0, n1};
+
+  double out[6];
+#pragma unroll
+  for (int f = 0; f < 6; f++) out[f] = (MODE == SMAUG_INT_EULER) ? T.s(f, lxo, lyo) : 0.0;
+
+  // velocities for the background coupling terms (computevel3)
+  if (P.has_bg) {
+    for (int r = tid; r < RC; r += NTHREADS) {
+      int lx = r % RX, ly = r / RX;
+      double rt = T.S[RHO * RC + r] + T.S[RHOB * RC + r];
+      T.X[5 * RC + r] = T.S[M1 * RC + r] / rt;
+      T.X[6 * RC + r] = T.S[M2 * RC + r] / rt;
+      (void)lx; (void)ly;
+    }
+  }
+
+  // ---- fluxes and divergence, per direction (centdiff1 / centdiff2) ------
+  for (int d = 0; d < 2; d++) {
+    // flux region: halo 2 along d, tile extent across
+    const int ex = (d == 0) ? TX + 4 : TX, ey = (d == 0) ? TY : TY + 4;
+    const int ox = (d == 0) ? 1 : HALO, oy = (d == 0) ? HALO : 1;
+    for (int r = tid; r < ex * ey; r += NTHREADS) {
+      int lx = ox + r % ex, ly = oy + r / ex;
+      int ci = T.x0 - HALO + lx, cj = T.y0 - HALO + ly;
+      double F[5] = {0, 0, 0, 0, 0};
+      if (ci >= 0 && ci < n0 && cj >= 0 && cj < n1) {
+        double v[NF2];
+        load_cell(T, lx, ly, v);
+        fluxes2(P.gamma, v, d, F);
+      }
+#pragma unroll
+      for (int k = 0; k < 5; k++) T.x(k, lx, ly) = F[k];
+    }
+    __syncthreads();
+    if (active) {
+      const int a = gidx[d], n = nn[d];
+      const int sx = (d == 0), sy = (d == 1);
+      const double dl = B.delx[d][a];
+      const bool z = (P.bt[d] != 0) && zero3dn(a, n);
+      const int fld[5] = {RHO, M1, M2, EN, (d == 0) ? B2 : B1};
+#pragma unroll
+      for (int k = 0; k < 5; k++) {
+        double fp1 = T.x(k, lxo + sx, lyo + sy), fm1 = T.x(k, lxo - sx, lyo - sy);
+        double fp2 = T.x(k, lxo + 2 * sx, lyo + 2 * sy), fm2 = T.x(k, lxo - 2 * sx, lyo - 2 * sy);
+        double g = ((8 * fp1 - 8 * fm1 + fm2 - fp2) / 6.0) / (2.0 * dl);
+        if (z) g = 0;
+        out[fld[k]] = out[fld[k]] - dt * g;
+        if (k == 3 && P.has_bg) {
+          // addenergyterms_cd2 (src/centdiff2.cu:80-115)
+          const double eb = T.s(EB, lxo, lyo), bb1 = T.s(BB1, lxo, lyo), bb2 = T.s(BB2, lxo, lyo);
+          const double ptb = (P.gamma - 1) * eb - 0.5 * (P.gamma - 2) * (bb1 * bb1 + bb2 * bb2);
+          const int vk = 5 + d;
+          double gv;
+          {
+            double a1 = T.x(vk, lxo + sx, lyo + sy), a_1 = T.x(vk, lxo - sx, lyo - sy);
+            double a2 = T.x(vk, lxo + 2 * sx, lyo + 2 * sy), a_2 = T.x(vk, lxo - 2 * sx, lyo - 2 * sy);
+            gv = ((8 * a1 - 8 * a_1 + a_2 - a2) / 6.0) / (2.0 * dl);
+            if (z) gv = 0;
+          }
+          out[EN] -= +(dt)*ptb * gv;
+          const double bbd = (d == 0) ? bb1 : bb2;
+#pragma unroll
+          for (int idim = 0; idim < 2; idim++) {
+            const int tx2 = (idim == 0), ty2 = (idim == 1);
+            const int ai = gidx[idim], ni = nn[idim];
+            double a1 = T.x(vk, lxo + tx2, lyo + ty2), a_1 = T.x(vk, lxo - tx2, lyo - ty2);
+            double a2 = T.x(vk, lxo + 2 * tx2, lyo + 2 * ty2), a_2 = T.x(vk, lxo - 2 * tx2, lyo - 2 * ty2);
+            double gi2 = ((8 * a1 - 8 * a_1 + a_2 - a2) / 6.0) / (2.0 * B.delx[idim][ai]);
+            if ((P.bt[idim] != 0) && zero3dn(ai, ni)) gi2 = 0;
+            const double bbi = (idim == 0) ? bb1 : bb2;
+            out[EN] += (dt)*bbi * bbd * gi2;
+          }
+        }
+      }
+    }
+    __syncthreads();
+  }
+
+  // ---- gravity (addgrav_cd2, src/centdiff2.cu:118-154) --------------------
+  if (P.has_grav && active) {
+    const double rho = T.s(RHO, lxo, lyo), rhob = T.s(RHOB, lxo, lyo);
+    out[M1] += (dt) * (P.g[0]) * rho;
+    out[M2] += (dt) * (P.g[1]) * rho;
+    out[EN] += (dt)*rho * ((P.g[0]) * T.s(M1, lxo, lyo)) / (rho + rhob);
+    out[EN] += (dt)*rho * ((P.g[1]) * T.s(M2, lxo, lyo)) / (rho + rhob);
+  }
+
+  // ---- hyperdiffusion ------------------------------------------------------
+  if (P.hyperdif == 1) {
+    // pass list in the driver's order (src/iosmaug.c:696-810):
+    // kind 0 rho, 1 energy, 2 momentum component, 3 B component
+    const int npass = 10;
+    const int pk[npass] = {0, 0, 1, 1, 2, 2, 2, 2, 3, 3};
+    const int pc[npass] = {0, 0, 0, 0, 0, 1, 0, 1, 1, 0};
+    const int pd[npass] = {0, 1, 0, 1, 0, 0, 1, 1, 0, 1};
+    for (int ip = 0; ip < npass; ip++) {
+      const int kind = pk[ip], comp = pc[ip], dim = pd[ip];
+      const int qfield = (kind == 0) ? RHO : (kind == 1) ? EN : (kind == 2) ? M1 + comp : B1 + comp;
+      const double coef = B.cmax_in[dim];
+      const double chyp = P.chyp[qfield];
+      const int sx = (dim == 0), sy = (dim == 1);
+      const int nd_ = nn[dim];
+      // (A) q over the tile, halo 3 along dim, 1 across
+      {
+        const int ex = (dim == 0) ? RX : TX + 2, ey = (dim == 0) ? TY + 2 : RY;
+        const int ox = (dim == 0) ? 0 : HALO - 1, oy = (dim == 0) ? HALO - 1 : 0;
+        for (int r = tid; r < ex * ey; r += NTHREADS) {
+          int lx = ox + r % ex, ly = oy + r / ex;
+          int ci = T.x0 - HALO + lx, cj = T.y0 - HALO + ly;
+          int a = (dim == 0) ? ci : cj, tr = (dim == 0) ? cj : ci, ntr = (dim == 0) ? n1 : n0;
+          double q = 0.0;
+          if (tr >= 0 && tr < ntr) {
+            if (a >= 0 && a < nd_) {
+              double v[NF2];
+              load_cell(T, lx, ly, v);
+              q = hq2(kind, comp, v);
+            } else if (a == -1) {
+              // left pad: bc_hyperdifl copies index 5 (src/hyperdifvisc1l.cu:30-44)
+              int l5x = (dim == 0) ? lx + 6 : lx, l5y = (dim == 0) ? ly : ly + 6;
+              double v[NF2];
+              load_cell(T, l5x, l5y, v);
+              q = hq2(kind, comp, v);
+            } else if (a == nd_) {
+              // right pad: stray tmp6 store of hyperdifvisc1r_parallel
+              int src = B.padsrc[dim][tr];
+              if (src >= 0) {
+                double v[NF2];
+#pragma unroll
+                for (int f = 0; f < 6; f++) v[f] = B.uin[f * nc + src];
+#pragma unroll
+                for (int f = 0; f < 4; f++) v[6 + f] = B.bg[f * nc + src];
+                q = hq2(kind, comp, v);
+              }
+            }
+          }
+          T.x(0, lx, ly) = q;
+        }
+      }
+      __syncthreads();
+      // (B) nu_r, nu_l on the tile and one cell across (hyperdifvisc2-4)
+      {
+        const int ex = (dim == 0) ? TX : TX + 2, ey = (dim == 0) ? TY + 2 : TY;
+        const int ox = (dim == 0) ? HALO : HALO - 1, oy = (dim == 0) ? HALO - 1 : HALO;
+        for (int r = tid; r < ex * ey; r += NTHREADS) {
+          int lx = ox + r % ex, ly = oy + r / ex;
+          int ci = T.x0 - HALO + lx, cj = T.y0 - HALO + ly;
+          double nur = 0.0, nul = 0.0;
+          if (ci >= 2 && ci <= n0 - 3 && cj >= 2 && cj <= n1 - 3) {
+            double q[8];  // q(a-3 .. a+4)
+#pragma unroll
+            for (int s = 0; s < 7; s++) q[s] = T.x(0, lx + (s - 3) * sx, ly + (s - 3) * sy);
+            q[7] = 0.0;
+            // faces f+1/2, f = a-3 .. a+2 ; D3 needs f-1..f+2
+            double d1[6], d3[4];
+#pragma unroll
+            for (int k = 0; k < 6; k++) d1[k] = fabs(q[k + 1] - q[k]);          // f = a-3+k
+#pragma unroll
+            for (int k = 0; k < 4; k++)                                        // f = a-2+k
+              d3[k] = fabs(3.0 * (q[k + 2] - q[k + 1]) - (q[k + 3] - q[k]));
+            double t4r = 0, t5r = 0, t4l = 0, t5l = 0;
+            t4r = dmax0(t4r, d3[1]); t4r = dmax0(t4r, d3[2]); t4r = dmax0(t4r, d3[3]);
+            t4l = dmax0(t4l, d3[0]); t4l = dmax0(t4l, d3[1]); t4l = dmax0(t4l, d3[2]);
+#pragma unroll
+            for (int k = 1; k < 6; k++) t5r = dmax0(t5r, d1[k]);
+#pragma unroll
+            for (int k = 0; k < 5; k++) t5l = dmax0(t5l, d1[k]);
+            const int a = (dim == 0) ? ci : cj;
+            const double dl = B.delx[dim][a];
+            if (t5r > 0) nur = dl * (coef) * (chyp) * t4r / t5r;
+            if (t5l > 0) nul = dl * (coef) * (chyp) * t4l / t5l;
+          }
+          T.x(1, lx, ly) = nur;
+          T.x(2, lx, ly) = nul;
+        }
+      }
+      __syncthreads();
+      // (C) cross-term arrays on the tile and one cell across
+      const bool cross = (kind == 2 && comp != dim) || (kind == 3);
+      if (cross) {
+        const int ex = (dim == 0) ? TX : TX + 2, ey = (dim == 0) ? TY + 2 : TY;
+        const int ox = (dim == 0) ? HALO : HALO - 1, oy = (dim == 0) ? HALO - 1 : HALO;
+        for (int r = tid; r < ex * ey; r += NTHREADS) {
+          int lx = ox + r % ex, ly = oy + r / ex;
+          int ci = T.x0 - HALO + lx, cj = T.y0 - HALO + ly;
+          double c3 = 0.0, c4 = 0.0;
+          if (ci >= 0 && ci < n0 && cj >= 0 && cj < n1) {
+            const int a = (dim == 0) ? ci : cj;
+            double g = 0.0;
+            if (ci > 0 && ci < n0 - 1 && cj > 0 && cj < n1 - 1) {
+              // grad13n (src/gradops.cu:755-823)
+              g = ((T.x(0, lx + sx, ly + sy) - T.x(0, lx - sx, ly - sy)) / (B.delx[dim][a])) / 2.0;
+              if ((P.bt[dim] != 0) && zero1n(a, nd_)) g = 0;
+            }
+            const double nur = T.x(1, lx, ly), nul = T.x(2, lx, ly);
+            if (kind == 2) {
+              // hyperdifmomsourcene2-4 (src/hyperdifmomsourcene1.cu:325-565)
+              double tau = g * ((nur + nul + 2.0 * 0.0)) / 4.0;
+              c3 = (T.s(RHO, lx, ly) + T.s(RHOB, lx, ly)) * tau;
+              c4 = tau * T.s(M1 + dim, lx, ly);
+            } else {
+              // hyperdifbsourcene1b-4 (src/hyperdifbsourcene1.cu:290-598)
+              double t3 = g * (nul + nur) / 2;
+              c3 = t3;
+              c4 = t3 * T.s(B1 + dim, lx, ly);
+            }
+          }
+          T.x(3, lx, ly) = c3;
+          T.x(4, lx, ly) = c4;
+        }
+        __syncthreads();
+      }
+      // (D) apply the sources at the tile cells
+      if (active) {
+        const int a = gidx[dim];
+        const double dl = B.delx[dim][a];
+        const double rdx = dl;
+        const double nur = T.x(1, lxo, lyo), nul = T.x(2, lxo, lyo);
+        const double q0 = T.x(0, lxo, lyo), qp = T.x(0, lxo + sx, lyo + sy), qm = T.x(0, lxo - sx, lyo - sy);
+        const bool z1 = (P.bt[dim] != 0) && zero1n(a, nd_);
+        double gr = (qp - q0) / (dl);   // grad1r3n
+        double gl = (q0 - qm) / (dl);   // grad1l3n
+        if (z1) { gr = 0; gl = 0; }
+        if (kind == 0) {
+          out[RHO] = out[RHO] + dt * ((nur + 0.0) * gr - (nul + 0.0) * gl) / rdx;
+        } else if (kind == 1) {
+          out[EN] = out[EN] + dt * ((nur + 0.0) * gr - (nul + 0.0) * gl) / rdx;
+        } else if (kind == 2) {
+          // hyperdifmomsource1-3a (src/hyperdifmomsource1.cu:17-511), ii0 = comp
+          const double r0 = T.s(RHO, lxo, lyo), rb0 = T.s(RHOB, lxo, lyo);
+          const double t2 = (r0 + rb0 + T.s(RHO, lxo - sx, lyo - sy) + T.s(RHOB, lxo - sx, lyo - sy)) / 2;
+          const double t3 = (r0 + rb0 + T.s(RHO, lxo + sx, lyo + sy) + T.s(RHOB, lxo + sx, lyo + sy)) / 2;
+          const double mf = T.s(M1 + comp, lxo, lyo);
+          const double t5 = (mf + T.s(M1 + comp, lxo - sx, lyo - sy)) / 2;
+          const double t6 = (mf + T.s(M1 + comp, lxo + sx, lyo + sy)) / 2;
+          const double dm = (t3 * (nur + 0.0) * gr - t2 * (nul + 0.0) * gl) / (rdx) / 2;
+          const double de = (t6 * (nur + 0.0) * gr - t5 * (nul + 0.0) * gl) / (rdx) / 2;
+          out[M1 + comp] = out[M1 + comp] + dt * dm;
+          out[EN] = out[EN] + dt * de;
+          if (comp == dim) {
+            out[M1 + comp] = out[M1 + comp] + dt * dm;
+            out[EN] = out[EN] + dt * de;
+          } else {
+            // hyperdifmomsourcene5-6a: d/dx_comp of (rho_t tau) and (tau m_dim)
+            const int f = comp, fx = (f == 0), fy = (f == 1);
+            const int af = gidx[f];
+            const double dlf = B.delx[f][af];
+            double g7 = ((T.x(3, lxo + fx, lyo + fy) - T.x(3, lxo - fx, lyo - fy)) / (dlf)) / 2.0;
+            double g8 = ((T.x(4, lxo + fx, lyo + fy) - T.x(4, lxo - fx, lyo - fy)) / (dlf)) / 2.0;
+            if ((P.bt[f] != 0) && zero1n(af, nn[f])) { g7 = 0; g8 = 0; }
+            out[M1 + dim] = out[M1 + dim] + dt * g7;
+            out[EN] = out[EN] + dt * g8;
+          }
+        } else {
+          // B component comp, diffused along dim != comp
+          // hyperdifbsourcene (jj=dim, ii0=dim, mm=comp, sb=-1)
+          const int f = comp, fx = (f == 0), fy = (f == 1);
+          const int af = gidx[f];
+          const double dlf = B.delx[f][af];
+          double g4 = ((T.x(3, lxo + fx, lyo + fy) - T.x(3, lxo - fx, lyo - fy)) / (dlf)) / 2.0;
+          double g6 = ((T.x(4, lxo + fx, lyo + fy) - T.x(4, lxo - fx, lyo - fy)) / (dlf)) / 2.0;
+          if ((P.bt[f] != 0) && zero1n(af, nn[f])) { g4 = 0; g6 = 0; }
+          out[B1 + dim] = out[B1 + dim] + dt * (-1.0 * g4);
+          out[EN] = out[EN] + dt * (-1.0 * g6);
+          // hyperdifbsource (jj=comp, ii0=comp, mm=dim, sb=+1)
+          const double t2 = (q0 + qm) / 2, t3 = (q0 + qp) / 2;
+          const double dB = 1.0 * (gr * nur - gl * nul) / rdx;
+          const double de = 1.0 * (t3 * gr * nur - t2 * gl * nul) / rdx;
+          out[B1 + comp] = out[B1 + comp] + dt * dB;
+          out[EN] = out[EN] + dt * de;
+        }
+      }
+      __syncthreads();
+    }
+  }
+
+  // ---- user driver (source_parallel + addsourceterms2) ---------------------
+  if (P.driver == SMAUG_DRIVER_GAUSS && active) {
+    double v = P.drv_amp;
+    if (P.drv_period > 0) v *= sin(tstage * 2.0 * M_PI / P.drv_period);
+    for (int d = 0; d < 2; d++) {
+      if (P.drv_sigma[d] > 0) {
+        double x = B.pos[d][gidx[d]] - P.drv_x0[d];
+        v *= exp(-x * x / (P.drv_sigma[d] * P.drv_sigma[d]));
+      }
+    }
+    const double rr = (MODE == SMAUG_INT_EULER) ? out[RHO] : T.s(RHO, lxo, lyo);
+    out[M1] = out[M1] + (dt)*v * (rr + T.s(RHOB, lxo, lyo));
+  }
+
+  // ---- combine, write, ghost images, CFL maxima -----------------------------
+  double cm[2] = {0.0, 0.0};
+  if (active) {
+    double res[6];
+    const long c = (long)gj * n0 + gi;
+    if (MODE == SMAUG_INT_EULER) {
+#pragma unroll
+      for (int f = 0; f < 6; f++) res[f] = out[f];
+    } else {
+      const double wgt = (B.stage == 0 || B.stage == 3) ? 1.0 / 6.0 : 1.0 / 3.0;
+      const double cst = (B.stage == 2) ? 1.0 : 0.5;
+#pragma unroll
+      for (int f = 0; f < 6; f++) {
+        const double dl = out[f];
+        if (B.stage == 0) {
+          const double u = T.s(f, lxo, lyo);
+          B.acc[f * nc + c] = u + wgt * dl;
+          res[f] = u + cst * dl;
+        } else if (B.stage < 3) {
+          B.acc[f * nc + c] = B.acc[f * nc + c] + wgt * dl;
+          res[f] = B.un[f * nc + c] + cst * dl;
+        } else {
+          res[f] = B.acc[f * nc + c] + wgt * dl;
+        }
+      }
+    }
+    bool bad = false;
+#pragma unroll
+    for (int f = 0; f < 6; f++) bad |= !isfinite(res[f]);
+    if (bad) atomicOr(B.flags, 1);
+    int ix[3], iy[3];
+    ix[0] = gi;
+    iy[0] = gj;
+    int nx = 1 + ghost_images(gi, n0, P.bc[0], ix + 1);
+    int ny = 1 + ghost_images(gj, n1, P.bc[1], iy + 1);
+    for (int b = 0; b < ny; b++)
+      for (int a = 0; a < nx; a++) {
+        const long cc = (long)iy[b] * n0 + ix[a];
+#pragma unroll
+        for (int f = 0; f < 6; f++) B.uout[f * nc + cc] = res[f];
+        double eb, rb, b1b, b2b;
+        if (a == 0 && b == 0) {
+          eb = T.s(EB, lxo, lyo); rb = T.s(RHOB, lxo, lyo); b1b = T.s(BB1, lxo, lyo); b2b = T.s(BB2, lxo, lyo);
+        } else {
+          eb = B.bg[0 * nc + cc]; rb = B.bg[1 * nc + cc]; b1b = B.bg[2 * nc + cc]; b2b = B.bg[3 * nc + cc];
+        }
+#pragma unroll
+        for (int d = 0; d < 2; d++) {
+          double cf = cfast2(P.gamma, res[RHO], res[M1], res[M2], res[EN], res[B1], res[B2], eb, rb, b1b,
+                             b2b, d);
+          cm[d] = dmax0(cm[d], cf);
+        }
+      }
+  }
+  // block max -> atomicMax (non-negative doubles order like their bit patterns)
+  __shared__ double red[NTHREADS / 32][2];
+#pragma unroll
+  for (int d = 0; d < 2; d++) {
+    double v = cm[d];
+    for (int o = 16; o > 0; o >>= 1) v = dmax0(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if ((tid & 31) == 0) red[tid >> 5][d] = v;
+  }
+  __syncthreads();
+  if (tid < 2) {
+    double v = 0.0;
+    for (int w = 0; w < NTHREADS / 32; w++) v = dmax0(v, red[w][tid]);
+    atomicMax(&B.cmax_out[tid], (unsigned long long)__double_as_longlong(v));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// auxiliary kernels: ghost fill and CFL maxima of an arbitrary state
+// ---------------------------------------------------------------------------
+// source interior index of a ghost index (inverse of ghost_images)
+__device__ __forceinline__ int ghost_source(int a, int n, int type) {
+  if (a >= 2 && a <= n - 3) return a;
+  switch (type) {
+    case SMAUG_BC_PERIODIC: return (a < 2) ? n - 4 + a : a - n + 4;
+    case SMAUG_BC_CONTCD4: return (a < 2) ? 4 - a : (a == n - 1 ? n - 5 : n - 4);
+    case SMAUG_BC_CONT: return (a < 2) ? 2 : n - 3;
+    case SMAUG_BC_SYMM: return (a < 2) ? 3 - a : 2 * n - 5 - a;
+    default: return a;
+  }
+}
+
+__global__ void ghost_fill2d_kernel(const KParams P, double* u) {
+  long c = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (c >= P.ncell) return;
+  int i = (int)(c % P.n0), j = (int)(c / P.n0);
+  int si = ghost_source(i, P.n0, P.bc[0]);
+  int sj = ghost_source(j, P.n1, P.bc[1]);
+  if (si == i && sj == j) return;
+  long s = (long)sj * P.n0 + si;
+  for (int f = 0; f < 6; f++) u[f * P.ncell + c] = u[f * P.ncell + s];
+}
+
+__global__ void cmax2d_kernel(const KParams P, const double* u, const double* bg,
+                              unsigned long long* out) {
+  long c = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  double cm[2] = {0, 0};
+  if (c < P.ncell) {
+    const long nc = P.ncell;
+    for (int d = 0; d < 2; d++)
+      cm[d] = cfast2(P.gamma, u[0 * nc + c], u[1 * nc + c], u[2 * nc + c], u[3 * nc + c],
+                     u[4 * nc + c], u[5 * nc + c], bg[0 * nc + c], bg[1 * nc + c], bg[2 * nc + c],
+                     bg[3 * nc + c], d);
+  }
+  for (int d = 0; d < 2; d++) {
+    double v = cm[d];
+    if (!(v > 0)) v = 0.0;
+    for (int o = 16; o > 0; o >>= 1) v = dmax0(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(&out[d], (unsigned long long)__double_as_longlong(v));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host engine
+// ---------------------------------------------------------------------------
+struct Engine {
+  smaug_params_t P{};
+  KParams K{};
+  int nd = 2, nevo = 6, nbg = 4;
+  long ncell = 0;
+  cudaStream_t stream = nullptr;
+  double* d_u[3] = {nullptr, nullptr, nullptr};
+  double* d_acc = nullptr;
+  double* d_bg = nullptr;
+  double* d_delx[3] = {nullptr, nullptr, nullptr};
+  double* d_pos[3] = {nullptr, nullptr, nullptr};
+  int* d_pad[3] = {nullptr, nullptr, nullptr};
+  unsigned long long* d_cmax = nullptr;  // ring of 3 x [3]
+  double* d_dt = nullptr;                // [2]
+  double* d_t = nullptr;                 // [2]
+  int* d_flags = nullptr;
+  std::vector<double> pos_host;          // positions after the metric rewrite
+  int cur = 0;                           // buffer holding the current state
+  long stage_count = 0;                  // launches so far (cmax ring position)
+  int parity = 0;                        // dt/t double buffer
+  int64_t it = 0;
+  int device = 0;
+};
+
+static void free_engine(Engine* e) {
+  if (!e) return;
+  for (int i = 0; i < 3; i++) {
+    cudaFree(e->d_u[i]);
+    cudaFree(e->d_delx[i]);
+    cudaFree(e->d_pos[i]);
+    cudaFree(e->d_pad[i]);
+  }
+  cudaFree(e->d_acc);
+  cudaFree(e->d_bg);
+  cudaFree(e->d_cmax);
+  cudaFree(e->d_dt);
+  cudaFree(e->d_t);
+  cudaFree(e->d_flags);
+  if (e->stream) cudaStreamDestroy(e->stream);
+  delete e;
+}
+
+static int validate(const smaug_params_t* p) {
+  if (!p) return set_error(SMAUG_E_INVALID, "null parameter block");
+  if (p->version != SMAUG_PARAMS_VERSION)
+    return set_error(SMAUG_E_INVALID, "parameter block version %d, expected %d", p->version,
+                     SMAUG_PARAMS_VERSION);
+  if (p->ndim == 3) return set_error(SMAUG_E_UNSUPPORTED, "3D is not implemented in this build");
+  if (p->ndim != 2) return set_error(SMAUG_E_INVALID, "ndim must be 2 or 3 (got %d)", p->ndim);
+  for (int d = 0; d < p->ndim; d++)
+    if (p->n[d] < 9) return set_error(SMAUG_E_INVALID, "n[%d]=%d: need at least 5 interior cells", d, p->n[d]);
+  if (p->integrator != SMAUG_INT_EULER && p->integrator != SMAUG_INT_RK4)
+    return set_error(SMAUG_E_INVALID, "unknown integrator %d", p->integrator);
+  if (p->precision != SMAUG_PREC_FP64)
+    return set_error(SMAUG_E_UNSUPPORTED, "precision form %d not implemented", p->precision);
+  if (p->pad_model != SMAUG_PAD_STRAY && p->pad_model != SMAUG_PAD_ZERO)
+    return set_error(SMAUG_E_INVALID, "unknown pad model %d", p->pad_model);
+  for (int d = 0; d < p->ndim; d++) {
+    int b = p->boundtype[d][0];
+    if (b != p->boundtype[d][1])
+      return set_error(SMAUG_E_UNSUPPORTED, "dim %d: different upper/lower boundary types", d);
+    if (b != SMAUG_BC_PERIODIC && b != SMAUG_BC_CONTCD4 && b != SMAUG_BC_CONT && b != SMAUG_BC_SYMM)
+      return set_error(SMAUG_E_UNSUPPORTED, "dim %d: boundary type %d not supported", d, b);
+  }
+  if (p->moddton == 1 && !(p->courant > 0))
+    return set_error(SMAUG_E_INVALID, "courant must be > 0 with moddton");
+  if (!(p->gamma > 1.0)) return set_error(SMAUG_E_INVALID, "gamma must be > 1");
+  if (p->driver != SMAUG_DRIVER_NONE && p->driver != SMAUG_DRIVER_GAUSS)
+    return set_error(SMAUG_E_INVALID, "unknown driver %d", p->driver);
+  return SMAUG_OK;
+}
+
+// Source cells of the stray tmp6 stores that land in the right pad along
+// each dim (src/hyperdifvisc1r.cu:1235,1255): the store of cell t goes to
+// linear index t + off of the padded array (off = n0+1 in 2D,
+// n0*n1+n0+1 in 3D); the pad cell of transverse row r along dim d is
+// padded (n_d+1) with the other coordinates +1.
+static std::vector<int> pad_sources(const smaug_params_t* p, int dim) {
+  int nd = p->ndim;
+  long n[3] = {p->n[0], p->n[1], nd == 3 ? p->n[2] : 1};
+  long m[3] = {n[0] + 2, n[1] + 2, nd == 3 ? n[2] + 2 : 1};
+  long dimp = n[0] * n[1] * n[2];
+  long off = (nd == 3) ? n[0] * n[1] + n[0] + 1 : n[0] + 1;
+  std::vector<int> src;
+  if (nd == 2) {
+    int o = 1 - dim;
+    src.assign(n[o], -1);
+    for (long r = 0; r < n[o]; r++) {
+      long P0 = (dim == 0) ? n[0] + 1 : r + 1;
+      long P1 = (dim == 0) ? r + 1 : n[1] + 1;
+      long L = P1 * m[0] + P0;
+      long t = L - off;
+      if (p->pad_model == SMAUG_PAD_STRAY && t >= 0 && t < dimp) src[r] = (int)t;
+    }
+  }
+  return src;
+}
+
+static int create(const smaug_params_t* p, const double* w, const double* pos, Engine** out) {
+  int rc = validate(p);
+  if (rc) return rc;
+  if (!w || !pos || !out) return set_error(SMAUG_E_INVALID, "null array argument");
+  Engine* e = new Engine();
+  e->P = *p;
+  e->nd = p->ndim;
+  e->nevo = 2 + 2 * e->nd;
+  e->nbg = 2 + e->nd;
+  e->ncell = 1;
+  for (int d = 0; d < e->nd; d++) e->ncell *= p->n[d];
+  const long nc = e->ncell;
+  const int nvar = 4 + 3 * e->nd;
+  // grid metric on the host (initgrid), then 1D metric arrays
+  e->pos_host.assign(pos, pos + (size_t)e->nd * nc);
+  std::vector<double> delx((size_t)e->nd * nc);
+  grid_metric(e->nd, p->n, e->pos_host.data(), delx.data());
+  std::vector<double> dl1[3], ps1[3];
+  for (int d = 0; d < e->nd; d++) {
+    dl1[d].assign(p->n[d], 0.0);
+    ps1[d].assign(p->n[d], 0.0);
+    // representative interior line; every interior cell must agree
+    int rep[2] = {2, 2};
+    for (int a = 0; a < p->n[d]; a++) {
+      int ij[2] = {rep[0], rep[1]};
+      ij[d] = a;
+      long c = (long)ij[1] * p->n[0] + ij[0];
+      dl1[d][a] = delx[(size_t)d * nc + c];
+      ps1[d][a] = e->pos_host[(size_t)d * nc + c];
+    }
+    for (int j = 2; j <= p->n[1] - 3; j++)
+      for (int i = 2; i <= p->n[0] - 3; i++) {
+        long c = (long)j * p->n[0] + i;
+        int a = (d == 0) ? i : j;
+        if (delx[(size_t)d * nc + c] != dl1[d][a] ||
+            (p->driver != SMAUG_DRIVER_NONE && e->pos_host[(size_t)d * nc + c] != ps1[d][a])) {
+          delete e;
+          return set_error(SMAUG_E_UNSUPPORTED,
+                           "grid metric along dim %d varies across lines (cell %d,%d); only "
+                           "tensor-product grids are supported", d, i, j);
+        }
+        if (!(dl1[d][a] > 0)) {
+          delete e;
+          return set_error(SMAUG_E_INVALID, "non-positive cell width along dim %d at %d", d, a);
+        }
+      }
+  }
+  // kernel parameters
+  KParams& K = e->K;
+  K.n0 = p->n[0];
+  K.n1 = p->n[1];
+  K.ncell = nc;
+  for (int d = 0; d < 3; d++) {
+    K.bt[d] = (d < e->nd) ? p->boundtype[d][0] : 0;
+    K.bc[d] = (d < e->nd) ? p->boundtype[d][0] : 0;
+    K.dx[d] = p->dx[d];
+    K.g[d] = p->g[d];
+    K.drv_x0[d] = p->drv_x0[d];
+    K.drv_sigma[d] = p->drv_sigma[d];
+  }
+  K.gamma = p->gamma;
+  K.courant = p->courant;
+  K.dtmax = p->dtmax;
+  for (int f = 0; f < SMAUG_MAXVAR; f++) K.chyp[f] = p->chyp[f];
+  K.moddton = p->moddton;
+  K.hyperdif = p->hyperdifmom;
+  K.has_grav = 0;
+  for (int d = 0; d < e->nd; d++) if (p->g[d] != 0.0) K.has_grav = 1;
+  K.has_bg = 0;
+  for (int f = 2 + 2 * e->nd; f < nvar; f++)
+    if (f != 3 + 2 * e->nd)  // rhob does not enter the coupling terms
+      for (long c = 0; c < nc; c++)
+        if (w[(size_t)f * nc + c] != 0.0) { K.has_bg = 1; break; }
+  K.driver = p->driver;
+  K.drv_amp = p->drv_amp;
+  K.drv_period = p->drv_period;
+  // device buffers
+  int dev = 0;
+  cudaGetDevice(&dev);
+  e->device = dev;
+  auto fail = [&](int code) { free_engine(e); return code; };
+#define E_TRY(call)                                                                             \
+  do {                                                                                          \
+    cudaError_t _e = (call);                                                                    \
+    if (_e != cudaSuccess)                                                                      \
+      return fail(set_error(_e == cudaErrorMemoryAllocation ? SMAUG_E_NOMEM : SMAUG_E_CUDA,    \
+                            "%s: %s", #call, cudaGetErrorString(_e)));                         \
+  } while (0)
+  E_TRY(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
+  size_t evo_bytes = sizeof(double) * e->nevo * nc;
+  for (int i = 0; i < 3; i++) E_TRY(cudaMalloc(&e->d_u[i], evo_bytes));
+  E_TRY(cudaMalloc(&e->d_acc, evo_bytes));
+  E_TRY(cudaMalloc(&e->d_bg, sizeof(double) * e->nbg * nc));
+  for (int d = 0; d < e->nd; d++) {
+    E_TRY(cudaMalloc(&e->d_delx[d], sizeof(double) * p->n[d]));
+    E_TRY(cudaMalloc(&e->d_pos[d], sizeof(double) * p->n[d]));
+    E_TRY(cudaMemcpy(e->d_delx[d], dl1[d].data(), sizeof(double) * p->n[d], cudaMemcpyHostToDevice));
+    E_TRY(cudaMemcpy(e->d_pos[d], ps1[d].data(), sizeof(double) * p->n[d], cudaMemcpyHostToDevice));
+    std::vector<int> ps = pad_sources(p, d);
+    E_TRY(cudaMalloc(&e->d_pad[d], sizeof(int) * ps.size()));
+    E_TRY(cudaMemcpy(e->d_pad[d], ps.data(), sizeof(int) * ps.size(), cudaMemcpyHostToDevice));
+  }
+  E_TRY(cudaMalloc(&e->d_cmax, sizeof(unsigned long long) * 9));
+  E_TRY(cudaMalloc(&e->d_dt, sizeof(double) * 2));
+  E_TRY(cudaMalloc(&e->d_t, sizeof(double) * 2));
+  E_TRY(cudaMalloc(&e->d_flags, sizeof(int)));
+  E_TRY(cudaMemcpy(e->d_u[0], w, evo_bytes, cudaMemcpyHostToDevice));
+  E_TRY(cudaMemcpy(e->d_bg, w + (size_t)e->nevo * nc, sizeof(double) * e->nbg * nc,
+                   cudaMemcpyHostToDevice));
+  double dt0[2] = {p->dt, p->dt}, t0[2] = {0.0, 0.0};
+  E_TRY(cudaMemcpy(e->d_dt, dt0, sizeof(dt0), cudaMemcpyHostToDevice));
+  E_TRY(cudaMemcpy(e->d_t, t0, sizeof(t0), cudaMemcpyHostToDevice));
+  E_TRY(cudaMemset(e->d_flags, 0, sizeof(int)));
+  E_TRY(cudaFuncSetAttribute(stage2d_kernel<SMAUG_INT_EULER>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM2D));
+  E_TRY(cudaFuncSetAttribute(stage2d_kernel<SMAUG_INT_RK4>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM2D));
+#undef E_TRY
+  *out = e;
+  return SMAUG_OK;
+}
+
+// ghost fill of the current state + CFL maxima into ring slot of the next launch
+static int reset_derived(Engine* e) {
+  const int bs = 256;
+  long nb = (e->ncell + bs - 1) / bs;
+  ghost_fill2d_kernel<<<(unsigned)nb, bs, 0, e->stream>>>(e->K, e->d_u[e->cur]);
+  CUDA_TRY(cudaGetLastError());
+  CUDA_TRY(cudaMemsetAsync(e->d_cmax, 0, sizeof(unsigned long long) * 9, e->stream));
+  unsigned long long* slot = e->d_cmax + 3 * (e->stage_count % 3);
+  cmax2d_kernel<<<(unsigned)nb, bs, 0, e->stream>>>(e->K, e->d_u[e->cur], e->d_bg, slot);
+  CUDA_TRY(cudaGetLastError());
+  return SMAUG_OK;
+}
+
+static int launch_stage(Engine* e, int mode, int stage, const double* uin, const double* un, double* uout) {
+  KBufs B{};
+  B.uin = uin;
+  B.un = un;
+  B.uout = uout;
+  B.acc = e->d_acc;
+  B.bg = e->d_bg;
+  for (int d = 0; d < 3; d++) {
+    B.delx[d] = e->d_delx[d];
+    B.pos[d] = e->d_pos[d];
+    B.padsrc[d] = e->d_pad[d];
+  }
+  long s = e->stage_count;
+  B.cmax_in = reinterpret_cast<const double*>(e->d_cmax + 3 * (s % 3));
+  B.cmax_out = e->d_cmax + 3 * ((s + 1) % 3);
+  B.cmax_clear = e->d_cmax + 3 * ((s + 2) % 3);
+  B.dt_prev = e->d_dt + e->parity;
+  B.dt_new = e->d_dt + (1 - e->parity);
+  B.t_prev = e->d_t + e->parity;
+  B.t_new = e->d_t + (1 - e->parity);
+  B.flags = e->d_flags;
+  B.mode = mode;
+  B.stage = stage;
+  dim3 block(TX, TY);
+  dim3 grid((e->K.n0 - 4 + TX - 1) / TX, (e->K.n1 - 4 + TY - 1) / TY);
+  if (mode == SMAUG_INT_EULER)
+    stage2d_kernel<SMAUG_INT_EULER><<<grid, block, SMEM2D, e->stream>>>(e->K, B);
+  else
+    stage2d_kernel<SMAUG_INT_RK4><<<grid, block, SMEM2D, e->stream>>>(e->K, B);
+  CUDA_TRY(cudaGetLastError());
+  e->stage_count++;
+  return SMAUG_OK;
+}
+
+static int step(Engine* e, int nsteps) {
+  for (int s = 0; s < nsteps; s++) {
+    int rc;
+    if (e->P.integrator == SMAUG_INT_EULER) {
+      int nxt = (e->cur + 1) % 3;
+      rc = launch_stage(e, SMAUG_INT_EULER, 0, e->d_u[e->cur], e->d_u[e->cur], e->d_u[nxt]);
+      if (rc) return rc;
+      e->cur = nxt;
+    } else {
+      int a = (e->cur + 1) % 3, b = (e->cur + 2) % 3;
+      double* un = e->d_u[e->cur];
+      if ((rc = launch_stage(e, SMAUG_INT_RK4, 0, un, un, e->d_u[a]))) return rc;
+      if ((rc = launch_stage(e, SMAUG_INT_RK4, 1, e->d_u[a], un, e->d_u[b]))) return rc;
+      if ((rc = launch_stage(e, SMAUG_INT_RK4, 2, e->d_u[b], un, e->d_u[a]))) return rc;
+      if ((rc = launch_stage(e, SMAUG_INT_RK4, 3, e->d_u[a], un, un))) return rc;
+    }
+    e->parity = 1 - e->parity;
+    e->it++;
+  }
+  CUDA_TRY(cudaStreamSynchronize(e->stream));
+  int flags = 0;
+  CUDA_TRY(cudaMemcpy(&flags, e->d_flags, sizeof(int), cudaMemcpyDeviceToHost));
+  if (flags & 1) return set_error(SMAUG_E_NONFINITE, "non-finite value in the evolved state by step %lld",
+                                  (long long)e->it);
+  return SMAUG_OK;
+}
+
+}  // namespace smaug
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+using smaug::Engine;
+
+extern "C" const char* smaug_last_error(void) { return smaug::last_error(); }
+extern "C" const char* smaug_version(void) { return SMAUG_VERSION_STRING; }
+
+extern "C" int smaug_params_default(smaug_params_t* p, int32_t ndim) {
+  smaug::clear_error();
+  if (!p || (ndim != 2 && ndim != 3)) return smaug::set_error(SMAUG_E_INVALID, "bad arguments");
+  memset(p, 0, sizeof(*p));
+  p->version = SMAUG_PARAMS_VERSION;
+  p->ndim = ndim;
+  p->n[0] = p->n[1] = 132;
+  p->n[2] = (ndim == 3) ? 132 : 1;
+  p->moddton = 1;
+  p->hyperdifmom = 1;
+  p->integrator = SMAUG_INT_EULER;
+  p->precision = SMAUG_PREC_FP64;
+  p->pad_model = SMAUG_PAD_STRAY;
+  for (int d = 0; d < 3; d++) p->dx[d] = (d < ndim) ? 2.0 * M_PI / 128.0 : 0.0;
+  p->dt = 1.0e-8;
+  p->dtmax = 1.0;
+  p->courant = 0.3;
+  p->gamma = 5.0 / 3.0;
+  for (int f = 0; f < SMAUG_MAXVAR; f++) p->chyp[f] = 0.2;
+  return SMAUG_OK;
+}
+
+extern "C" int smaug_create(const smaug_params_t* p, const double* w, const double* pos,
+                            smaug_handle_t* out) {
+  smaug::clear_error();
+  if (!out) return smaug::set_error(SMAUG_E_INVALID, "null handle pointer");
+  *out = nullptr;
+  Engine* e = nullptr;
+  int rc = smaug::create(p, w, pos, &e);
+  if (rc) return rc;
+  rc = smaug::reset_derived(e);
+  if (!rc) {
+    cudaError_t ce = cudaStreamSynchronize(e->stream);
+    if (ce != cudaSuccess) rc = smaug::set_error(SMAUG_E_CUDA, "create: %s", cudaGetErrorString(ce));
+  }
+  if (rc) {
+    smaug::free_engine(e);
+    return rc;
+  }
+  *out = reinterpret_cast<smaug_handle_t>(e);
+  return SMAUG_OK;
+}
+
+static Engine* H(smaug_handle_t h) { return reinterpret_cast<Engine*>(h); }
+
+extern "C" int smaug_step(smaug_handle_t h, int32_t nsteps) {
+  smaug::clear_error();
+  if (!h) return smaug::set_error(SMAUG_E_INVALID, "null handle");
+  if (nsteps < 0) return smaug::set_error(SMAUG_E_INVALID, "nsteps < 0");
+  return smaug::step(H(h), nsteps);
+}
+
+extern "C" int smaug_get_state(smaug_handle_t h, double* w) {
+  smaug::clear_error();
+  if (!h || !w) return smaug::set_error(SMAUG_E_INVALID, "null argument");
+  Engine* e = H(h);
+  CUDA_TRY(cudaStreamSynchronize(e->stream));
+  CUDA_TRY(cudaMemcpy(w, e->d_u[e->cur], sizeof(double) * e->nevo * e->ncell, cudaMemcpyDeviceToHost));
+  CUDA_TRY(cudaMemcpy(w + (size_t)e->nevo * e->ncell, e->d_bg, sizeof(double) * e->nbg * e->ncell,
+                      cudaMemcpyDeviceToHost));
+  return SMAUG_OK;
+}
+
+extern "C" int smaug_set_state(smaug_handle_t h, const double* w) {
+  smaug::clear_error();
+  if (!h || !w) return smaug::set_error(SMAUG_E_INVALID, "null argument");
+  Engine* e = H(h);
+  CUDA_TRY(cudaStreamSynchronize(e->stream));
+  CUDA_TRY(cudaMemcpy(e->d_u[e->cur], w, sizeof(double) * e->nevo * e->ncell, cudaMemcpyHostToDevice));
+  int rc = smaug::reset_derived(e);
+  if (rc) return rc;
+  CUDA_TRY(cudaStreamSynchronize(e->stream));
+  return SMAUG_OK;
+}
+
+extern "C" int smaug_get_time(smaug_handle_t h, int64_t* it, double* t, double* dt) {
+  smaug::clear_error();
+  if (!h) return smaug::set_error(SMAUG_E_INVALID, "null handle");
+  Engine* e = H(h);
+  CUDA_TRY(cudaStreamSynchronize(e->stream));
+  double tb[2], db[2];
+  CUDA_TRY(cudaMemcpy(tb, e->d_t, sizeof(tb), cudaMemcpyDeviceToHost));
+  CUDA_TRY(cudaMemcpy(db, e->d_dt, sizeof(db), cudaMemcpyDeviceToHost));
+  if (it) *it = e->it;
+  if (t) *t = tb[e->parity];
+  if (dt) *dt = db[e->parity];
+  return SMAUG_OK;
+}
+
+extern "C" int smaug_get_cmax(smaug_handle_t h, double* cmax) {
+  smaug::clear_error();
+  if (!h || !cmax) return smaug::set_error(SMAUG_E_INVALID, "null argument");
+  Engine* e = H(h);
+  CUDA_TRY(cudaStreamSynchronize(e->stream));
+  double c[3];
+  CUDA_TRY(cudaMemcpy(c, e->d_cmax + 3 * (e->stage_count % 3), sizeof(c), cudaMemcpyDeviceToHost));
+  for (int d = 0; d < e->nd; d++) cmax[d] = c[d];
+  return SMAUG_OK;
+}
+
+extern "C" int smaug_write_out(smaug_handle_t h, const char* path, const char* name, int32_t it,
+                               double t) {
+  smaug::clear_error();
+  if (!h || !path) return smaug::set_error(SMAUG_E_INVALID, "null argument");
+  Engine* e = H(h);
+  std::vector<double> w((size_t)(e->nevo + e->nbg) * e->ncell);
+  int rc = smaug_get_state(h, w.data());
+  if (rc) return rc;
+  return smaug::write_out_host(path, &e->P, w.data(), e->pos_host.data(), name, it, t);
+}
+
+extern "C" int smaug_destroy(smaug_handle_t h) {
+  smaug::clear_error();
+  if (!h) return SMAUG_OK;
+  Engine* e = H(h);
+  cudaStreamSynchronize(e->stream);
+  smaug::free_engine(e);
+  return SMAUG_OK;
+}

@@ -1,0 +1,172 @@
+"""Python binding of the engine's C ABI (include/smaug_b200.h).
+
+Mirrors the reference's host flow (src/iosmaug.c): create from an initial
+state (cuinit + initgrid + boundaries), step, copy back (cuupdate), write
+.out snapshots (writevacconfig).  All compute runs in libsmaug_b200.so on the
+GPU; there is no CPU path.  Errors raise SmaugError with the library message.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+from . import params as _params
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIBPATH = os.path.join(HERE, "libsmaug_b200.so")
+
+EXPORTS = [
+    "smaug_params_default", "smaug_create", "smaug_step", "smaug_get_state",
+    "smaug_set_state", "smaug_get_time", "smaug_get_cmax", "smaug_write_out",
+    "smaug_destroy", "smaug_last_error", "smaug_version", "smaug_read_ini",
+    "smaug_write_out_host", "smaug_grid_metric",
+]
+
+ERRORS = {1: "invalid", 2: "cuda", 3: "nomem", 4: "io", 5: "format", 6: "unsupported",
+          7: "nonfinite"}
+
+
+class SmaugError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("smaug error %d (%s): %s" % (code, ERRORS.get(code, "?"), msg))
+        self.code = code
+
+
+_lib = None
+
+
+def lib():
+    """Load the engine library; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIBPATH):
+            raise ImportError("libsmaug_b200.so not built (run __graft_entry__.build() "
+                              "or python smaug_b200/build.py)")
+        L = ctypes.CDLL(LIBPATH)
+        dp = ctypes.POINTER(ctypes.c_double)
+        vp = ctypes.c_void_p
+        L.smaug_params_default.argtypes = [vp, ctypes.c_int32]
+        L.smaug_create.argtypes = [vp, dp, dp, ctypes.POINTER(vp)]
+        L.smaug_step.argtypes = [vp, ctypes.c_int32]
+        L.smaug_get_state.argtypes = [vp, dp]
+        L.smaug_set_state.argtypes = [vp, dp]
+        L.smaug_get_time.argtypes = [vp, ctypes.POINTER(ctypes.c_int64), dp, dp]
+        L.smaug_get_cmax.argtypes = [vp, dp]
+        L.smaug_write_out.argtypes = [vp, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int32,
+                                      ctypes.c_double]
+        L.smaug_destroy.argtypes = [vp]
+        L.smaug_last_error.restype = ctypes.c_char_p
+        L.smaug_version.restype = ctypes.c_char_p
+        L.smaug_read_ini.argtypes = [ctypes.c_char_p, ctypes.c_int32,
+                                     ctypes.POINTER(ctypes.c_int32), dp, dp,
+                                     ctypes.POINTER(ctypes.c_int32), dp]
+        L.smaug_write_out_host.argtypes = [ctypes.c_char_p, vp, dp, dp, ctypes.c_char_p,
+                                           ctypes.c_int32, ctypes.c_double]
+        L.smaug_grid_metric.argtypes = [ctypes.c_int32, ctypes.POINTER(ctypes.c_int32), dp, dp]
+        _lib = L
+    return _lib
+
+
+def _check(rc):
+    if rc:
+        raise SmaugError(rc, lib().smaug_last_error().decode())
+
+
+def _dp(a):
+    if a.dtype != np.float64 or not a.flags["C_CONTIGUOUS"]:
+        raise TypeError("expected a C-contiguous float64 array")
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def version():
+    return lib().smaug_version().decode()
+
+
+def grid_metric(ndim, n, pos):
+    """Host restatement of initgrid: returns (rewritten positions, delx)."""
+    pos = np.array(pos, dtype=np.float64, order="C")
+    delx = np.zeros_like(pos)
+    nn = (ctypes.c_int32 * 3)(*(list(n) + [1] * (3 - len(n))))
+    _check(lib().smaug_grid_metric(ndim, nn, _dp(pos), _dp(delx)))
+    return pos, delx
+
+
+def read_ini(path, ndim, n):
+    nvar = 4 + 3 * ndim
+    shape = tuple(reversed(list(n)[:ndim]))
+    w = np.zeros((nvar,) + shape)
+    pos = np.zeros((ndim,) + shape)
+    nn = (ctypes.c_int32 * 3)(*(list(n) + [1] * (3 - len(n))))
+    it = ctypes.c_int32(0)
+    t = ctypes.c_double(0.0)
+    _check(lib().smaug_read_ini(path.encode(), ndim, nn, _dp(w), _dp(pos), ctypes.byref(it),
+                                ctypes.byref(t)))
+    return w, pos, int(it.value), float(t.value)
+
+
+class Engine:
+    """One simulation on the current CUDA device."""
+
+    def __init__(self, params, w, pos):
+        self.p = params
+        self.shape = (params.nvar,) + params.shape
+        w = np.ascontiguousarray(w, dtype=np.float64)
+        pos = np.ascontiguousarray(pos, dtype=np.float64)
+        if w.shape != self.shape:
+            raise ValueError("state shape %s, expected %s" % (w.shape, self.shape))
+        if pos.shape != (params.ndim,) + params.shape:
+            raise ValueError("positions shape %s" % (pos.shape,))
+        h = ctypes.c_void_p()
+        _check(lib().smaug_create(ctypes.byref(params), _dp(w), _dp(pos), ctypes.byref(h)))
+        self.h = h
+
+    def step(self, n=1):
+        _check(lib().smaug_step(self.h, int(n)))
+        return self
+
+    def state(self):
+        w = np.zeros(self.shape)
+        _check(lib().smaug_get_state(self.h, _dp(w)))
+        return w
+
+    def set_state(self, w):
+        w = np.ascontiguousarray(w, dtype=np.float64)
+        _check(lib().smaug_set_state(self.h, _dp(w)))
+
+    def time(self):
+        it = ctypes.c_int64(0)
+        t = ctypes.c_double(0)
+        dt = ctypes.c_double(0)
+        _check(lib().smaug_get_time(self.h, ctypes.byref(it), ctypes.byref(t), ctypes.byref(dt)))
+        return int(it.value), float(t.value), float(dt.value)
+
+    def cmax(self):
+        c = np.zeros(3)
+        _check(lib().smaug_get_cmax(self.h, _dp(c)))
+        return c[: self.p.ndim]
+
+    def write_out(self, path, name="test1", it=None, t=None):
+        i, tt, _ = self.time()
+        _check(lib().smaug_write_out(self.h, path.encode(), name.encode(),
+                                     int(i if it is None else it), float(tt if t is None else t)))
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().smaug_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
+def make_params(**kw):
+    return _params.make_params(**kw)
