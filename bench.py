@@ -1,0 +1,325 @@
+"""Benchmark of the SMAUG time advance on B200 (one JSON line on rank 0).
+
+Workload (N=1): 2D Orszag-Tang vortex, 4096 x 4096 interior cells (+2 ghost
+layers), periodic, hyperdiffusion on, CFL 0.3, seeded 1e-3 rho noise, FP64,
+classical RK4 -- the bandwidth/roofline configuration of the benchmark suite.
+A step is one RK4 step (4 fused stage launches).  The state (0.8 GB per
+buffer) is far larger than the 126 MB L2, so no flush is needed between steps.
+
+  value  Mcell-updates/s per RK4 step, state resident in HBM, CUDA events on
+         the engine's stream (torch's current stream is handed to the engine)
+  e2e    the same metric through the C ABI with host buffers: per step
+         smaug_set_state (pinned H2D) + smaug_step + smaug_get_state (D2H)
+N>1 (torchrun): replicas only -- each rank advances its own copy, no
+collective on the data path; value = total cell updates / max rank time.
+
+--impl reference: the reference has no CPU solver (every routine is a CUDA
+kernel), so the CPU baseline is the oracle, the FP64 restatement of the
+reference's kernels (oracle/), run with all host threads on a bounded
+sample of the same workload.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD_N = 4096
+METRIC = "Mcell-updates/s per RK4 step"
+UNIT = "Mcell-updates/s"
+# algorithmic HBM bytes per interior cell per RK4 step (FP64, 2D: P=6
+# evolved, B=4 background fields): stage 0 reads Un,B writes U2,Acc (3P+B);
+# stages 1-2 read Us,Un,Acc,B write Us+1,Acc (5P+B); stage 3 reads U4,Acc,B
+# writes Un+1 (3P+B) -> 16P+4B = 112 doubles
+ALG_BYTES_PER_CELL_STEP = (16 * 6 + 4 * 4) * 8
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        d = json.load(open(path))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks/throttle reasons during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index=0):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = threading.Thread(target=self._run, daemon=True)
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                                      "--format=csv,noheader,nounits"],
+                                     capture_output=True, text=True, timeout=5).stdout
+                for ln in out.strip().splitlines():
+                    f = [x.strip() for x in ln.split(",")]
+                    self.samples.append(f)
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for s in self.samples:
+            for k, nm in enumerate(names):
+                if len(s) > 5 + k and s[5 + k].lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.samples)}
+
+
+def make_case(N, seed=1):
+    from smaug_b200 import ic, params as P
+    w, pos, dx = ic.orszag_tang(N, noise=1e-3, seed=seed)
+    p = P.make_params(ndim=2, n=(N + 4, N + 4, 1), dx=dx, courant=0.3, dtmax=1.0,
+                      integrator=P.INT_RK4)
+    return p, w, pos
+
+
+def dist_setup(args):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import torch
+        import torch.distributed as dist
+        import datetime
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl" if args.impl != "reference" else "gloo",
+                                timeout=datetime.timedelta(seconds=300))
+    return ws, rank, local
+
+
+def cpu_sample(N=512, steps=1):
+    """Oracle (the reference arithmetic on CPU, all host threads) on a
+    bounded sample: `steps` RK4 steps of an N x N Orszag-Tang grid."""
+    from oracle import pyoracle
+    p, w, pos = make_case(N)
+    run = pyoracle.OracleRun(p, w, pos)
+    t0 = time.perf_counter()
+    run.advance(steps)
+    el = time.perf_counter() - t0
+    return N * N * steps / el / 1e6, el, pyoracle.num_threads()
+
+
+def reference_arm(args, ws, rank):
+    if rank != 0:
+        return
+    from oracle import build
+    build.build()
+    os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+    N = args.ref_sample
+    for _ in range(args.warmup):
+        cpu_sample(N, 1)
+    vals = []
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        v, el, thr = cpu_sample(N, 1)
+        vals.append(el)
+    total = time.perf_counter() - t0
+    value = N * N * args.steps / sum(vals) / 1e6
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * sum(vals) / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "2D Orszag-Tang %dx%d sample of the %dx%d workload, FP64, RK4"
+                   % (N, N, WORKLOAD_N, WORKLOAD_N), "parallelism": "cpu",
+                   "sample_cells": N * N},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": thr, "kind": "port",
+                         "sample": "%d RK4 steps of a %dx%d Orszag-Tang grid per measured "
+                                   "step; oracle/smaug_oracle.c (OpenMP)" % (1, N, N)},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "wall_s": total,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def reference_gpu_binary(timeout=240):
+    """Per-step time of the reference's own GPU binary (built from its
+    sources by oracle/build_ref.py, Euler, 1024^2): Mcell-updates/s per
+    Euler step from its own 'time total' lines, first 5 steps discarded."""
+    binp = os.path.join(ROOT, "oracle", "_ref", "ot1024t", "smaug")
+    if not os.path.exists(binp):
+        return None
+    import tempfile
+    from smaug_b200 import formats
+    from oracle import run_ref
+    p, w, pos = make_case(1024)
+    d = tempfile.mkdtemp(prefix="refbin_")
+    ini = os.path.join(d, "in.ini")
+    formats.write_ini(ini, w, pos)
+    try:
+        rc, times = run_ref.run(binp, ini, os.path.join(d, "run"), keep=set(), timeout=timeout)
+    except Exception as e:  # noqa: BLE001
+        return {"error": str(e)}
+    if rc != 0 or len(times) < 8:
+        return {"error": "rc=%s steps=%d" % (rc, len(times))}
+    tt = [t for s, t in times]
+    per = (tt[-1] - tt[4]) / (len(tt) - 5)
+    return {"value": 1024 * 1024 / per / 1e6, "unit": "Mcell-updates/s per Euler step",
+            "ms_per_step": per * 1e3, "workload": "2D Orszag-Tang 1024x1024, FP64, Euler",
+            "kind": "reference binary built from source, its own per-step timer"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=WORKLOAD_N)
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--ref-sample", type=int, default=512)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-ref-gpu", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    ws, rank, local = dist_setup(args)
+    if args.impl == "reference":
+        reference_arm(args, ws, rank)
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+
+    import numpy as np
+    import torch
+    from smaug_b200 import engine
+
+    torch.cuda.set_device(local)
+    N = args.n
+    p, w, pos = make_case(N, seed=1 + rank)
+    eng = engine.Engine(p, w, pos)
+    # a dedicated stream: the engine launches on it, the events are recorded on it
+    stream = torch.cuda.Stream()
+    assert stream.cuda_stream != 0
+    eng.set_stream(stream.cuda_stream)
+    ncell_int = N * N
+
+    def barrier():
+        if ws > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    # warm-up
+    eng.step_async(args.warmup)
+    eng.sync()
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        eng.step_async(args.steps)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    eng.sync()
+    barrier()
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if ws > 1:
+        import torch.distributed as dist
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = ncell_int * args.steps * ws / (ms_max / 1e3) / 1e6
+    launches = 4 * args.steps
+
+    # e2e: host buffers through the C ABI, pinned memory, copies in the timed region
+    nvar = p.nvar
+    host = torch.empty((nvar,) + p.shape, dtype=torch.float64, pin_memory=True).numpy()
+    eng.state(out=host)
+    barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.e2e_steps):
+        eng.set_state(host)      # H2D of the evolved fields
+        eng.step(1)
+        eng.state(out=host)      # D2H of the whole state (reference cuupdate)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    te = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
+    if ws > 1:
+        import torch.distributed as dist
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_ms = float(te.item())
+    e2e_val = ncell_int * args.e2e_steps * ws / (e2e_ms / 1e3) / 1e6
+    h2d = 6 * p.ncells * 8
+    d2h = nvar * p.ncells * 8
+    eng.close()
+
+    if rank == 0:
+        peak, pk_kind = peaks()
+        achieved = ALG_BYTES_PER_CELL_STEP * ncell_int * args.steps / (ms / 1e3) / 1e9
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "2D Orszag-Tang %dx%d (+2 ghost layers), periodic, "
+                                   "hyperdiffusion, CFL 0.3, FP64, classical RK4" % (N, N),
+                       "interior_cells": ncell_int, "integrator": "rk4", "precision": "fp64",
+                       "parallelism": "replicas" if ws > 1 else "single-gpu",
+                       "l2": "state 0.8 GB per buffer > 126 MB L2, no flush"},
+            "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "steps": args.e2e_steps,
+                    "path": "smaug_set_state + smaug_step + smaug_get_state, pinned host buffers",
+                    "gpu_launches_per_step": 4 + 2},
+            "gpu_launches": launches,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None,
+                         "peak_kind": pk_kind,
+                         "alg_bytes_per_cell_step": ALG_BYTES_PER_CELL_STEP,
+                         "note": "stage kernel; FP64 arithmetic, not HBM, limits this form"},
+            "clocks": clk.summary(),
+        }
+        if ws == 1 and not args.no_cpu_baseline:
+            os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+            v, el, thr = cpu_sample(args.ref_sample, 1)
+            line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": thr, "kind": "port",
+                                    "sample": "1 RK4 step of a %dx%d Orszag-Tang grid (%.1f s), "
+                                              "oracle/smaug_oracle.c, OpenMP" % (
+                                                  args.ref_sample, args.ref_sample, el)}
+        if ws == 1 and not args.no_ref_gpu:
+            line["reference_gpu"] = reference_gpu_binary()
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -62,8 +62,13 @@ extern "C" {
 /* precision forms */
 #define SMAUG_PREC_FP64 0
 
-/* fill model for the right-biased hyperdiffusion pad (see DESIGN) */
-#define SMAUG_PAD_STRAY 0  /* pad holds the stray tmp6 store, as observed */
+/* Fill model of the outer layer of the padded array from which the
+   reference's right-biased hyperviscosity is computed.  hyperdifvisc1r_parallel
+   (src/hyperdifvisc1r.cu:1099-1258) zeroes that array and, in the same
+   launch, stores tmp6 through encode3 instead of encode3p2; the stray stores
+   that land in the pad race with the zeroing.  Inside a 512-thread block the
+   stray store lands last, which is what the reference produced on a B200. */
+#define SMAUG_PAD_STRAY 0  /* pad holds the stray tmp6 store */
 #define SMAUG_PAD_ZERO 1   /* pad holds zero */
 
 /* user source (driver) kinds */
@@ -124,6 +129,19 @@ int smaug_create(const smaug_params_t* p, const double* w, const double* pos,
 /* Advance nsteps steps.  Replaces the body of the step loop
    src/iosmaug.c:496-1144 (cucomputedervfields ... cuboundary). */
 int smaug_step(smaug_handle_t h, int32_t nsteps);
+
+/* Enqueue nsteps steps on the engine's stream without waiting; the
+   non-finite check is reported by the next smaug_sync.  For capture in CUDA
+   graphs and for timing with events on the caller's stream. */
+int smaug_step_async(smaug_handle_t h, int32_t nsteps);
+
+/* Wait for the engine's stream; returns SMAUG_E_NONFINITE if a NaN/Inf was
+   produced since the last check. */
+int smaug_sync(smaug_handle_t h);
+
+/* Launch on `stream` (a cudaStream_t) from now on; NULL restores the
+   engine's own stream.  The caller keeps ownership of the stream. */
+int smaug_set_stream(smaug_handle_t h, void* stream);
 
 /* Copy the current state (all NVAR fields, ghosts included) to the host.
    Replaces cuupdate (src/update.cu:165-233). */

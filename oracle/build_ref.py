@@ -79,6 +79,11 @@ def build_ref(name, ni, nj, nt, arch="sm_100a", verbose=True, **kw):
     cfg.update({k.upper(): str(v) for k, v in kw.items()})
     dest = os.path.join(OUT, name)
     os.makedirs(dest, exist_ok=True)
+    stamp = "ni=%d nj=%d nt=%d %s arch=%s\n" % (ni, nj, nt, sorted(cfg.items()), arch)
+    binp = os.path.join(dest, "smaug")
+    stampf = os.path.join(dest, "build.txt")
+    if os.path.exists(binp) and os.path.exists(stampf) and open(stampf).read() == stamp:
+        return binp
     tmp = tempfile.mkdtemp(prefix="smaug_ref_")
     try:
         for d in ("src", "include", "models"):
@@ -132,16 +137,32 @@ def build_ref(name, ni, nj, nt, arch="sm_100a", verbose=True, **kw):
                 print(" ".join(cmd), flush=True)
             subprocess.check_call(cmd, cwd=src)
             objs.append(o)
-        binp = os.path.join(dest, "smaug")
         cmd = ["nvcc", "-arch=" + arch, "-o", binp] + objs + ["-lcudart", "-lm"]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.check_call(cmd, cwd=src)
-        with open(os.path.join(dest, "build.txt"), "w") as f:
-            f.write("ni=%d nj=%d nt=%d %s\n" % (ni, nj, nt, cfg))
+        with open(stampf, "w") as f:
+            f.write(stamp)
         return binp
     finally:
         shutil.rmtree(tmp, ignore_errors=True)
+
+
+# Binaries used by tests/golden/make_golden.py (single-block grids, every
+# step saved) and by bench.py's reference-GPU timing line (1024^2, no
+# per-step output).
+STANDARD = [
+    ("g16", 16, 16, 21, {}),
+    ("g18x12", 18, 12, 21, {}),
+    ("ot1024t", 1024, 1024, 12, {"PCFGSAVEFREQUENCY": "100000"}),
+]
+
+
+def build_standard(verbose=False):
+    out = {}
+    for name, ni, nj, nt, kw in STANDARD:
+        out[name] = build_ref(name, ni, nj, nt, verbose=verbose, **kw)
+    return out
 
 
 if __name__ == "__main__":

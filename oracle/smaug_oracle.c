@@ -262,10 +262,6 @@ static double grad13n(const O *o, const double *a, const int *ii, int dir) {
 /* ---- derived fields (src/dervfields.cu) ------------------------------- */
 #define W(f) (w[F(o, (f)) + c])
 
-static double rhot(const O *o, const double *w, long c) {
-  return W(o->rho) + W(o->rhob);
-}
-
 /* computevel3_MODID, src/dervfields.cu:79-98 */
 static void computevel3(O *o, const double *w, long c) {
   for (int d = 0; d < o->nd; d++)
@@ -1265,7 +1261,8 @@ int or_cmax(const smaug_params_t *P, const double *w, double *cmaxd) {
  *   state  in/out: [0]=p->dt (previous dt), [1]=t (simulated time)
  *   cmax_out  per-dim CFL maxima of the last step input (may be NULL)
  * integrator: SMAUG_INT_EULER reproduces the reference step; SMAUG_INT_RK4
- * is classical RK4 on the same operator (dt and stage cmax as in DESIGN).
+ * is classical RK4 on the same operator: dt from the CFL maxima of the step
+ * input, each stage evaluated with the CFL maxima of its own input.
  */
 int or_advance(const smaug_params_t *P, double *w, const double *pos,
                const double *delx, int nsteps, double *state, double *cmax_out) {
@@ -1304,6 +1301,7 @@ int or_advance(const smaug_params_t *P, double *w, const double *pos,
       static const double wgt[4] = {1.0 / 6.0, 1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0};
       memcpy(un, w, sizeof(double) * nw);
       memcpy(ustage, w, sizeof(double) * nw);
+      memcpy(acc, w, sizeof(double) * nw); /* carries the background fields */
       double t0 = o.t;
       double dt = 0;
       for (int st = 0; st < 4; st++) {

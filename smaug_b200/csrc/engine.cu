@@ -742,6 +742,7 @@ struct Engine {
   int parity = 0;                        // dt/t double buffer
   int64_t it = 0;
   int device = 0;
+  cudaStream_t own_stream = nullptr;     // created by the engine
 };
 
 static void free_engine(Engine* e) {
@@ -758,7 +759,7 @@ static void free_engine(Engine* e) {
   cudaFree(e->d_dt);
   cudaFree(e->d_t);
   cudaFree(e->d_flags);
-  if (e->stream) cudaStreamDestroy(e->stream);
+  if (e->own_stream) cudaStreamDestroy(e->own_stream);
   delete e;
 }
 
@@ -906,7 +907,8 @@ static int create(const smaug_params_t* p, const double* w, const double* pos, E
       return fail(set_error(_e == cudaErrorMemoryAllocation ? SMAUG_E_NOMEM : SMAUG_E_CUDA,    \
                             "%s: %s", #call, cudaGetErrorString(_e)));                         \
   } while (0)
-  E_TRY(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
+  E_TRY(cudaStreamCreateWithFlags(&e->own_stream, cudaStreamNonBlocking));
+  e->stream = e->own_stream;
   size_t evo_bytes = sizeof(double) * e->nevo * nc;
   for (int i = 0; i < 3; i++) E_TRY(cudaMalloc(&e->d_u[i], evo_bytes));
   E_TRY(cudaMalloc(&e->d_acc, evo_bytes));
@@ -987,7 +989,19 @@ static int launch_stage(Engine* e, int mode, int stage, const double* uin, const
   return SMAUG_OK;
 }
 
-static int step(Engine* e, int nsteps) {
+static int sync_check(Engine* e) {
+  CUDA_TRY(cudaStreamSynchronize(e->stream));
+  int flags = 0;
+  CUDA_TRY(cudaMemcpy(&flags, e->d_flags, sizeof(int), cudaMemcpyDeviceToHost));
+  if (flags & 1) {
+    CUDA_TRY(cudaMemset(e->d_flags, 0, sizeof(int)));
+    return set_error(SMAUG_E_NONFINITE, "non-finite value in the evolved state by step %lld",
+                     (long long)e->it);
+  }
+  return SMAUG_OK;
+}
+
+static int enqueue_steps(Engine* e, int nsteps) {
   for (int s = 0; s < nsteps; s++) {
     int rc;
     if (e->P.integrator == SMAUG_INT_EULER) {
@@ -1006,12 +1020,13 @@ static int step(Engine* e, int nsteps) {
     e->parity = 1 - e->parity;
     e->it++;
   }
-  CUDA_TRY(cudaStreamSynchronize(e->stream));
-  int flags = 0;
-  CUDA_TRY(cudaMemcpy(&flags, e->d_flags, sizeof(int), cudaMemcpyDeviceToHost));
-  if (flags & 1) return set_error(SMAUG_E_NONFINITE, "non-finite value in the evolved state by step %lld",
-                                  (long long)e->it);
   return SMAUG_OK;
+}
+
+static int step(Engine* e, int nsteps) {
+  int rc = enqueue_steps(e, nsteps);
+  if (rc) return rc;
+  return sync_check(e);
 }
 
 }  // namespace smaug
@@ -1074,6 +1089,28 @@ extern "C" int smaug_step(smaug_handle_t h, int32_t nsteps) {
   if (!h) return smaug::set_error(SMAUG_E_INVALID, "null handle");
   if (nsteps < 0) return smaug::set_error(SMAUG_E_INVALID, "nsteps < 0");
   return smaug::step(H(h), nsteps);
+}
+
+extern "C" int smaug_step_async(smaug_handle_t h, int32_t nsteps) {
+  smaug::clear_error();
+  if (!h) return smaug::set_error(SMAUG_E_INVALID, "null handle");
+  if (nsteps < 0) return smaug::set_error(SMAUG_E_INVALID, "nsteps < 0");
+  return smaug::enqueue_steps(H(h), nsteps);
+}
+
+extern "C" int smaug_sync(smaug_handle_t h) {
+  smaug::clear_error();
+  if (!h) return smaug::set_error(SMAUG_E_INVALID, "null handle");
+  return smaug::sync_check(H(h));
+}
+
+extern "C" int smaug_set_stream(smaug_handle_t h, void* stream) {
+  smaug::clear_error();
+  if (!h) return smaug::set_error(SMAUG_E_INVALID, "null handle");
+  Engine* e = H(h);
+  CUDA_TRY(cudaStreamSynchronize(e->stream));
+  e->stream = stream ? static_cast<cudaStream_t>(stream) : e->own_stream;
+  return SMAUG_OK;
 }
 
 extern "C" int smaug_get_state(smaug_handle_t h, double* w) {

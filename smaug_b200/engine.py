@@ -19,7 +19,8 @@ EXPORTS = [
     "smaug_params_default", "smaug_create", "smaug_step", "smaug_get_state",
     "smaug_set_state", "smaug_get_time", "smaug_get_cmax", "smaug_write_out",
     "smaug_destroy", "smaug_last_error", "smaug_version", "smaug_read_ini",
-    "smaug_write_out_host", "smaug_grid_metric",
+    "smaug_write_out_host", "smaug_grid_metric", "smaug_step_async", "smaug_sync",
+    "smaug_set_stream",
 ]
 
 ERRORS = {1: "invalid", 2: "cuda", 3: "nomem", 4: "io", 5: "format", 6: "unsupported",
@@ -48,6 +49,9 @@ def lib():
         L.smaug_params_default.argtypes = [vp, ctypes.c_int32]
         L.smaug_create.argtypes = [vp, dp, dp, ctypes.POINTER(vp)]
         L.smaug_step.argtypes = [vp, ctypes.c_int32]
+        L.smaug_step_async.argtypes = [vp, ctypes.c_int32]
+        L.smaug_sync.argtypes = [vp]
+        L.smaug_set_stream.argtypes = [vp, vp]
         L.smaug_get_state.argtypes = [vp, dp]
         L.smaug_set_state.argtypes = [vp, dp]
         L.smaug_get_time.argtypes = [vp, ctypes.POINTER(ctypes.c_int64), dp, dp]
@@ -124,8 +128,24 @@ class Engine:
         _check(lib().smaug_step(self.h, int(n)))
         return self
 
-    def state(self):
-        w = np.zeros(self.shape)
+    def step_async(self, n=1):
+        """Enqueue n steps on the engine's stream without waiting."""
+        _check(lib().smaug_step_async(self.h, int(n)))
+        return self
+
+    def sync(self):
+        _check(lib().smaug_sync(self.h))
+
+    def set_stream(self, stream_handle):
+        """Launch on the given cudaStream_t (an int handle, e.g.
+        torch.cuda.current_stream().cuda_stream); None restores the engine's own."""
+        _check(lib().smaug_set_stream(self.h, ctypes.c_void_p(stream_handle or None)))
+
+    def state(self, out=None):
+        """Copy the state to the host (into `out`, e.g. a pinned buffer, if given)."""
+        w = np.zeros(self.shape) if out is None else out
+        if w.shape != self.shape:
+            raise ValueError("out has shape %s, expected %s" % (w.shape, self.shape))
         _check(lib().smaug_get_state(self.h, _dp(w)))
         return w
 

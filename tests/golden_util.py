@@ -1,0 +1,32 @@
+"""Loading of the reference golden fixtures (tests/golden/*.npz)."""
+import os
+
+import numpy as np
+
+from smaug_b200 import params as P
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+STRICT = ("g16", "g18x12", "ot64")     # full multi-step runs
+ONESTEP = ("ot24x20",)                 # consecutive steps, one-step parity
+
+
+def load(name):
+    z = np.load(os.path.join(GOLDEN, name + ".npz"))
+    d = {k: z[k] for k in z.files}
+    w0 = np.zeros((10,) + d["w0"].shape[1:])
+    w0[:6] = d["w0"]
+    d["w0full"] = w0
+    return d
+
+
+def params(d, **kw):
+    ny, nx = d["w0"].shape[1:]
+    kw.setdefault("integrator", P.INT_EULER)
+    return P.make_params(ndim=2, n=(nx, ny, 1), dx=tuple(d["dx"]), gamma=float(d["gamma"]),
+                         courant=0.3, dtmax=1.0, dt=1e-8, **kw)
+
+
+def full(w6):
+    w = np.zeros((10,) + w6.shape[1:])
+    w[:6] = w6
+    return w

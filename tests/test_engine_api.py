@@ -1,0 +1,98 @@
+"""C-ABI behaviour: errors, state round trips, determinism, chunking,
+non-finite detection, .out output."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from smaug_b200 import formats, params as P
+from tests.util import ot_rect, params_for
+
+pytestmark = pytest.mark.gpu
+
+
+def test_invalid_params_rejected(engine_lib):
+    w, pos, dx = ot_rect(16, 16)
+    for kw, code in [({"integrator": 7}, 1), ({"pad_model": 9}, 1), ({"boundtype": (5, 0)}, 6),
+                     ({"gamma": 1.0}, 1)]:
+        p = params_for(w, dx, **kw)
+        with pytest.raises(engine_lib.SmaugError) as e:
+            engine_lib.Engine(p, w, pos)
+        assert e.value.code == code, kw
+    p = params_for(w, dx)
+    p.version = 99
+    with pytest.raises(engine_lib.SmaugError) as e:
+        engine_lib.Engine(p, w, pos)
+    assert e.value.code == 1
+    p = params_for(w, dx)
+    p.n[0] = 8
+    with pytest.raises((engine_lib.SmaugError, ValueError)):
+        engine_lib.Engine(p, w[:, :, :8].copy(), pos[:, :, :8].copy())
+
+
+def test_null_handle(engine_lib):
+    L = engine_lib.lib()
+    assert L.smaug_step(None, 1) == 1
+    assert L.smaug_destroy(None) == 0
+
+
+def test_state_roundtrip_and_determinism(engine_lib):
+    w, pos, dx = ot_rect(40, 33, seed=4)
+    p = params_for(w, dx, integrator=P.INT_RK4)
+    a = engine_lib.Engine(p, w, pos)
+    s0 = a.state()
+    assert np.array_equal(s0[6:], w[6:])
+    a.step(4)
+    b = engine_lib.Engine(p, w, pos)
+    b.step(1).step(3)
+    assert np.array_equal(a.state(), b.state())          # chunking
+    assert a.time() == b.time()
+    mid = a.state()
+    a.set_state(mid)
+    a.step(2)
+    b.step(2)
+    assert np.array_equal(a.state(), b.state())          # set_state is exact
+    a.close()
+    b.close()
+
+
+def test_zero_steps(engine_lib):
+    w, pos, dx = ot_rect(12, 12)
+    e = engine_lib.Engine(params_for(w, dx), w, pos)
+    s = e.state()
+    e.step(0)
+    assert np.array_equal(s, e.state())
+    assert e.time()[0] == 0
+
+
+def test_nonfinite_detected(engine_lib):
+    w, pos, dx = ot_rect(20, 20)
+    w[0, 10, 10] = np.nan
+    p = params_for(w, dx, moddton=0, dt=1e-3)
+    e = engine_lib.Engine(p, w, pos)
+    with pytest.raises(engine_lib.SmaugError) as err:
+        e.step(1)
+    assert err.value.code == 7
+    e.close()
+
+
+def test_write_out(engine_lib, tmp_path):
+    w, pos, dx = ot_rect(10, 9, seed=8)
+    p = params_for(w, dx)
+    e = engine_lib.Engine(p, w, pos)
+    e.step(2)
+    path = str(tmp_path / "s.out")
+    e.write_out(path, name="test1", it=2, t=0.5)
+    w2, pos2, hdr = formats.read_out(path)
+    assert np.array_equal(w2, e.state())
+    assert hdr["it"] == 2 and hdr["t"] == 0.5 and hdr["n"] == [14, 13]
+    e.close()
+
+
+def test_3d_reports_unsupported(engine_lib):
+    p = P.make_params(ndim=3, n=(12, 12, 12))
+    w = np.zeros((13, 12, 12, 12))
+    pos = np.zeros((3, 12, 12, 12))
+    with pytest.raises(engine_lib.SmaugError) as e:
+        engine_lib.Engine(p, w, pos)
+    assert e.value.code == 6
