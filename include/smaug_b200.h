@@ -172,6 +172,30 @@ const char* smaug_last_error(void);
 const char* smaug_version(void);
 
 /*
+ * One reference (Euler) step that allocates nothing.  No counterpart in the
+ * reference: it exists for callers that cannot call cudaMalloc -- code
+ * recording a CUDA graph by stream capture, hosts that own all device memory
+ * through their own pool or budget, loops that must not take the implicit
+ * synchronisation of an allocation.
+ *   w_in, w_out : DEVICE buffers, NVAR*ncells doubles each, reference layout;
+ *                 w_in needs valid ghost layers (as left by a previous step);
+ *                 w_out receives the whole state (backgrounds copied).
+ *   delx        : HOST array of n[0]+n[1] doubles, the cell widths along dim 0
+ *                 then dim 1 (one interior line of smaug_grid_metric's output).
+ *   dt          : HOST in/out: the previous step's dt in, this step's dt out.
+ *   stream      : cudaStream_t or NULL.
+ * 2D only, no driver term, at most 8192 cells per dimension (ghosts
+ * included); larger grids are rejected with SMAUG_E_UNSUPPORTED.  Scratch
+ * lives in one static device array of 196,864 bytes per GPU, kept until the
+ * process exits and shared by every call: calls whose GPU work overlaps (other
+ * threads or streams) race on it and must be serialised by the caller.  The
+ * first call on a device looks up that array's device address; make that
+ * first call before any stream capture.  Returns after the step completed.
+ */
+int smaug_euler_step_noalloc(const smaug_params_t* p, const double* w_in, double* w_out,
+                             const double* delx, double* dt, void* stream);
+
+/*
  * Format boundary (host only, no device use).
  * Read a reference ASCII .ini (src/readwrite.c:975-1082): header + one line
  * per cell "pos[ndim] w[nvar]".  n[] must be set by the caller (the reference

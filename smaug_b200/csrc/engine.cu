@@ -24,6 +24,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1178,5 +1179,164 @@ extern "C" int smaug_destroy(smaug_handle_t h) {
   Engine* e = H(h);
   cudaStreamSynchronize(e->stream);
   smaug::free_engine(e);
+  return SMAUG_OK;
+}
+
+// ===========================================================================
+// Allocation-free Euler step
+// ===========================================================================
+// Some callers cannot call cudaMalloc: code that records its work into a
+// CUDA graph by stream capture (allocation is not allowed while a capture is
+// active), hosts that hand the library memory they already own from their
+// own pool or a fixed device budget, and latency-critical loops where an
+// allocation's implicit device synchronisation would stall other streams.
+// smaug_euler_step_noalloc serves them: the caller passes device buffers for
+// the input and output state, and every piece of scratch the step needs (CFL
+// maxima, dt and time words, the error flag, the 1D metric and the stray-pad
+// source table) lives in the file-scope array below.
+namespace smaug {
+
+// Largest grid (cells per dimension, ghosts included) the array serves.
+constexpr int NOALLOC_MAXN = 8192;
+constexpr size_t NA_CMAX = 0;                                        // 9 x u64
+constexpr size_t NA_DT = 128;                                        // 2 doubles
+constexpr size_t NA_T = 160;                                         // 2 doubles
+constexpr size_t NA_FLAGS = 192;                                     // 1 int
+constexpr size_t NA_DELX = 256;                                      // 2 x MAXN doubles
+constexpr size_t NA_PAD = NA_DELX + 2 * NOALLOC_MAXN * sizeof(double);  // 2 x MAXN ints
+constexpr size_t NOALLOC_SCRATCH_BYTES = NA_PAD + 2 * NOALLOC_MAXN * sizeof(int);  // 196,864 B
+
+// One copy per GPU that loads the library, held until the process exits.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
+
+// Device address of g_noalloc_scratch per device (the host-side symbol is a
+// stand-in, not a device address); filled on a device's first call.
+constexpr int NA_MAXDEV = 64;
+static unsigned char* g_na_ptr[NA_MAXDEV] = {nullptr};
+static std::mutex g_na_mu;
+
+static int noalloc_scratch(unsigned char** out) {
+  int dev = 0;
+  CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= NA_MAXDEV) return set_error(SMAUG_E_UNSUPPORTED, "device %d out of range", dev);
+  std::lock_guard<std::mutex> lk(g_na_mu);
+  if (!g_na_ptr[dev]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess)
+      return set_error(SMAUG_E_CUDA, "cudaGetSymbolAddress(g_noalloc_scratch): %s", cudaGetErrorString(e));
+    g_na_ptr[dev] = static_cast<unsigned char*>(p);
+  }
+  *out = g_na_ptr[dev];
+  return SMAUG_OK;
+}
+
+// stray-pad source cells (same rule as pad_sources on the host) into scratch
+__global__ void noalloc_pad_kernel(int n0, int n1, int stray, int* pad0, int* pad1) {
+  int r = blockIdx.x * blockDim.x + threadIdx.x;
+  long dimp = (long)n0 * n1, off = n0 + 1;
+  if (r < n1) {  // dim 0: padded (n0+1, r+1)
+    long t = (long)(r + 1) * (n0 + 2) + (n0 + 1) - off;
+    pad0[r] = (stray && t >= 0 && t < dimp) ? (int)t : -1;
+  }
+  if (r < n0) {  // dim 1: padded (r+1, n1+1)
+    long t = (long)(n1 + 1) * (n0 + 2) + (r + 1) - off;
+    pad1[r] = (stray && t >= 0 && t < dimp) ? (int)t : -1;
+  }
+}
+
+}  // namespace smaug
+
+extern "C" int smaug_euler_step_noalloc(const smaug_params_t* p, const double* w_in, double* w_out,
+                                        const double* delx, double* dt, void* stream) {
+  using namespace smaug;
+  clear_error();
+  int rc = validate(p);
+  if (rc) return rc;
+  if (!w_in || !w_out || !delx || !dt) return set_error(SMAUG_E_INVALID, "null argument");
+  if (w_in == w_out) return set_error(SMAUG_E_INVALID, "w_in and w_out must not alias");
+  if (p->n[0] > NOALLOC_MAXN || p->n[1] > NOALLOC_MAXN)
+    return set_error(SMAUG_E_UNSUPPORTED,
+                     "grid %d x %d exceeds the allocation-free limit of %d cells per dimension",
+                     p->n[0], p->n[1], NOALLOC_MAXN);
+  if (p->driver != SMAUG_DRIVER_NONE)
+    return set_error(SMAUG_E_UNSUPPORTED, "the allocation-free step has no driver term");
+  unsigned char* s = nullptr;
+  if ((rc = noalloc_scratch(&s))) return rc;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const long nc = (long)p->n[0] * p->n[1];
+  // kernel parameters (same fields as Engine::K)
+  KParams K{};
+  K.n0 = p->n[0];
+  K.n1 = p->n[1];
+  K.ncell = nc;
+  for (int d = 0; d < 3; d++) {
+    K.bt[d] = (d < 2) ? p->boundtype[d][0] : 0;
+    K.bc[d] = K.bt[d];
+    K.dx[d] = p->dx[d];
+    K.g[d] = p->g[d];
+  }
+  K.gamma = p->gamma;
+  K.courant = p->courant;
+  K.dtmax = p->dtmax;
+  for (int f = 0; f < SMAUG_MAXVAR; f++) K.chyp[f] = p->chyp[f];
+  K.moddton = p->moddton;
+  K.hyperdif = p->hyperdifmom;
+  K.has_grav = (p->g[0] != 0.0 || p->g[1] != 0.0);
+  K.has_bg = 1;  // exact either way; no host pass over the state
+  K.driver = SMAUG_DRIVER_NONE;
+  unsigned long long* cm = reinterpret_cast<unsigned long long*>(s + NA_CMAX);
+  double* dtb = reinterpret_cast<double*>(s + NA_DT);
+  double* tb = reinterpret_cast<double*>(s + NA_T);
+  int* flags = reinterpret_cast<int*>(s + NA_FLAGS);
+  double* dl = reinterpret_cast<double*>(s + NA_DELX);
+  int* pad = reinterpret_cast<int*>(s + NA_PAD);
+  // the array keeps the previous call's contents: reset what must start at zero
+  CUDA_TRY(cudaMemsetAsync(s, 0, NA_DELX, st));
+  CUDA_TRY(cudaMemcpyAsync(dl, delx, sizeof(double) * p->n[0], cudaMemcpyHostToDevice, st));
+  CUDA_TRY(cudaMemcpyAsync(dl + NOALLOC_MAXN, delx + p->n[0], sizeof(double) * p->n[1],
+                           cudaMemcpyHostToDevice, st));
+  CUDA_TRY(cudaMemcpyAsync(dtb, dt, sizeof(double), cudaMemcpyHostToDevice, st));
+  int nmax = p->n[0] > p->n[1] ? p->n[0] : p->n[1];
+  noalloc_pad_kernel<<<(nmax + 255) / 256, 256, 0, st>>>(p->n[0], p->n[1],
+                                                         p->pad_model == SMAUG_PAD_STRAY, pad,
+                                                         pad + NOALLOC_MAXN);
+  CUDA_TRY(cudaGetLastError());
+  const double* bg = w_in + 6 * nc;
+  cmax2d_kernel<<<(unsigned)((nc + 255) / 256), 256, 0, st>>>(K, w_in, bg, cm);
+  CUDA_TRY(cudaGetLastError());
+  KBufs B{};
+  B.uin = w_in;
+  B.un = w_in;
+  B.uout = w_out;
+  B.acc = nullptr;
+  B.bg = bg;
+  B.delx[0] = dl;
+  B.delx[1] = dl + NOALLOC_MAXN;
+  B.padsrc[0] = pad;
+  B.padsrc[1] = pad + NOALLOC_MAXN;
+  B.cmax_in = reinterpret_cast<const double*>(cm);
+  B.cmax_out = cm + 3;
+  B.cmax_clear = cm + 6;
+  B.dt_prev = dtb;
+  B.dt_new = dtb + 1;
+  B.t_prev = tb;
+  B.t_new = tb + 1;
+  B.flags = flags;
+  B.mode = SMAUG_INT_EULER;
+  B.stage = 0;
+  CUDA_TRY(cudaFuncSetAttribute(stage2d_kernel<SMAUG_INT_EULER>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM2D));
+  dim3 block(TX, TY);
+  dim3 grid((p->n[0] - 4 + TX - 1) / TX, (p->n[1] - 4 + TY - 1) / TY);
+  stage2d_kernel<SMAUG_INT_EULER><<<grid, block, SMEM2D, st>>>(K, B);
+  CUDA_TRY(cudaGetLastError());
+  // background fields are constant: carry them to the output
+  CUDA_TRY(cudaMemcpyAsync(w_out + 6 * nc, bg, sizeof(double) * 4 * nc, cudaMemcpyDeviceToDevice, st));
+  int hflags = 0;
+  CUDA_TRY(cudaMemcpyAsync(dt, dtb + 1, sizeof(double), cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(cudaMemcpyAsync(&hflags, flags, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(cudaStreamSynchronize(st));
+  if (hflags & 1) return set_error(SMAUG_E_NONFINITE, "non-finite value in the evolved state");
   return SMAUG_OK;
 }

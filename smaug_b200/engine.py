@@ -20,7 +20,7 @@ EXPORTS = [
     "smaug_set_state", "smaug_get_time", "smaug_get_cmax", "smaug_write_out",
     "smaug_destroy", "smaug_last_error", "smaug_version", "smaug_read_ini",
     "smaug_write_out_host", "smaug_grid_metric", "smaug_step_async", "smaug_sync",
-    "smaug_set_stream",
+    "smaug_set_stream", "smaug_euler_step_noalloc",
 ]
 
 ERRORS = {1: "invalid", 2: "cuda", 3: "nomem", 4: "io", 5: "format", 6: "unsupported",
@@ -52,6 +52,7 @@ def lib():
         L.smaug_step_async.argtypes = [vp, ctypes.c_int32]
         L.smaug_sync.argtypes = [vp]
         L.smaug_set_stream.argtypes = [vp, vp]
+        L.smaug_euler_step_noalloc.argtypes = [vp, vp, vp, dp, dp, vp]
         L.smaug_get_state.argtypes = [vp, dp]
         L.smaug_set_state.argtypes = [vp, dp]
         L.smaug_get_time.argtypes = [vp, ctypes.POINTER(ctypes.c_int64), dp, dp]
@@ -186,6 +187,18 @@ class Engine:
 
     def __exit__(self, *a):
         self.close()
+
+
+def euler_step_noalloc(params, w_in_ptr, w_out_ptr, delx1d, dt, stream=None):
+    """One Euler step on caller-owned device buffers (integer device
+    pointers), allocating nothing; delx1d = widths along dim 0 then dim 1
+    (host); returns this step's dt."""
+    delx1d = np.ascontiguousarray(delx1d, dtype=np.float64)
+    d = ctypes.c_double(dt)
+    _check(lib().smaug_euler_step_noalloc(ctypes.byref(params), ctypes.c_void_p(w_in_ptr),
+                                          ctypes.c_void_p(w_out_ptr), _dp(delx1d),
+                                          ctypes.byref(d), ctypes.c_void_p(stream)))
+    return d.value
 
 
 def make_params(**kw):
