@@ -71,8 +71,6 @@ constexpr int RY = TY + 2 * HALO;
 constexpr int RC = RX * RY;
 constexpr int NTHREADS = TX * TY;
 constexpr int NF2 = 10;            // 2D fields: 6 evolved + 4 background
-constexpr int NSCR = 7;            // scratch arrays of RC doubles
-constexpr size_t SMEM2D = sizeof(double) * (size_t)(NF2 + NSCR) * RC;
 
 // 2D field ids (include/iotypes.h:209-216)
 enum { RHO = 0, M1 = 1, M2 = 2, EN = 3, B1 = 4, B2 = 5, EB = 6, RHOB = 7, BB1 = 8, BB2 = 9 };
@@ -194,484 +192,7 @@ __device__ __forceinline__ bool zero1n(int a, int n) {
 // ---------------------------------------------------------------------------
 // 2D stage kernel
 // ---------------------------------------------------------------------------
-struct Tile {
-  double* S;  // [NF2][RC]
-  double* X;  // [NSCR][RC]
-  int x0, y0;
-  __device__ __forceinline__ double& s(int f, int lx, int ly) const { return S[f * RC + ly * RX + lx]; }
-  __device__ __forceinline__ double& x(int k, int lx, int ly) const { return X[k * RC + ly * RX + lx]; }
-};
-
-// q of a hyperdiffusion pass (hyperdifvisc1r_parallel tmp6,
-// src/hyperdifvisc1r.cu:1225-1253) from the 10 field values
-__device__ __forceinline__ double hq2(int kind, int comp, const double* v) {
-  switch (kind) {
-    case 0:  // rho
-      return v[RHO];
-    case 1: {  // energy: e - (B'^2 + m^2/rho_t)/2
-      return v[EN] - 0.5 * ((v[B1] * v[B1] + v[B2] * v[B2]) +
-                            (v[M1] * v[M1] + v[M2] * v[M2]) / (v[RHO] + v[RHOB]));
-    }
-    case 2:  // velocity component
-      return v[M1 + comp] / ((v[RHO] + v[RHOB]));
-    default:  // magnetic perturbation component
-      return v[B1 + comp];
-  }
-}
-
-__device__ __forceinline__ double ptot2(double gamma, const double* v) {
-  // computept3 (src/dervfields.cu:107-153)
-  double pt = (gamma - 2.0) * ((v[B1] * v[BB1] + v[B2] * v[BB2]) + 0.5 * (v[B1] * v[B1] + v[B2] * v[B2]));
-  return (gamma - 1.0) * (v[EN] - 0.5 * (v[M1] * v[M1] + v[M2] * v[M2]) / (v[RHO] + v[RHOB])) - pt;
-}
-
-__device__ __forceinline__ void load_cell(const Tile& T, int lx, int ly, double* v) {
-#pragma unroll
-  for (int f = 0; f < NF2; f++) v[f] = T.s(f, lx, ly);
-}
-
-// fluxes along d of rho, m1, m2, e and the transverse B component
-// (src/centdiff1.cu:51-197, src/centdiff2.cu:203-323)
-__device__ __forceinline__ void fluxes2(double gamma, const double* v, int d, double* F) {
-  double rt = v[RHO] + v[RHOB];
-  double md = v[M1 + d];
-  double pt = ptot2(gamma, v);
-  // rho
-  F[0] = md * v[RHO] / rt + (v[RHOB] * md) / (v[RHOB] + v[RHO]);
-  // momentum components
-#pragma unroll
-  for (int c = 0; c < 2; c++) {
-    double bf = v[B1 + c], bbf = v[BB1 + c], bbd = v[BB1 + d], bd = v[B1 + d];
-    double fm = (d == c) ? pt - (bf * bbd + bbf * bd) - bf * bd : -(bf * bbd + bbf * bd) - bf * bd;
-    double x = 0.0;
-    x += md * v[M1 + c] / rt + fm;
-    F[1 + c] = x;
-  }
-  // energy
-  {
-    double bbm = v[BB1] * v[M1] + v[BB2] * v[M2];
-    double bm = v[B1] * v[M1] + v[B2] * v[M2];
-    double ft = md * (pt);
-    ft -= v[B1 + d] * bbm;
-    ft -= v[BB1 + d] * bm;
-    ft /= rt;
-    ft += md * v[EB] / rt;
-    ft -= v[B1 + d] * bm / rt;
-    F[3] = md * v[EN] / rt + ft;
-  }
-  // B component c != d
-  {
-    int c = 1 - d;
-    F[4] = md * v[B1 + c] / rt - (v[B1 + d] + v[BB1 + d]) * v[M1 + c] / rt +
-           (v[BB1 + c]) * v[M1 + d] / rt;
-  }
-}
-
-template <int MODE>
-__global__ void __launch_bounds__(NTHREADS, 2) stage2d_kernel(const KParams P, const KBufs B) {
-  extern __shared__ double smem[];
-  Tile T;
-  T.S = smem;
-  T.X = smem + NF2 * RC;
-  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
-  T.x0 = 2 + blockIdx.x * TX;
-  T.y0 = 2 + blockIdx.y * TY;
-  const int n0 = P.n0, n1 = P.n1;
-  const long nc = P.ncell;
-
-  // ---- stage the state tile ------------------------------------------
-  for (int r = tid; r < RC; r += NTHREADS) {
-    int lx = r % RX, ly = r / RX;
-    int gi = T.x0 - HALO + lx, gj = T.y0 - HALO + ly;
-    bool in = gi >= 0 && gi < n0 && gj >= 0 && gj < n1;
-    long c = (long)gj * n0 + gi;
-#pragma unroll
-    for (int f = 0; f < 6; f++) T.S[f * RC + r] = in ? B.uin[f * nc + c] : 0.0;
-#pragma unroll
-    for (int f = 0; f < 4; f++) T.S[(6 + f) * RC + r] = in ? B.bg[f * nc + c] : (f == 1 ? 1.0 : 0.0);
-  }
-
-  // ---- dt of this step and stage time ----------------------------------
-  double dt, tstage;
-  if (B.stage == 0) {
-    dt = device_dt(P, B.cmax_in, *B.dt_prev, 2);
-    if (blockIdx.x == 0 && blockIdx.y == 0 && tid == 0) {
-      *B.dt_new = dt;
-      *B.t_new = *B.t_prev + dt;
-      B.cmax_clear[0] = B.cmax_clear[1] = B.cmax_clear[2] = 0ull;
-    }
-    tstage = *B.t_prev;
-  } else {
-    dt = *B.dt_new;
-    tstage = *B.t_prev + (B.stage == 3 ? dt : 0.5 * dt);
-    if (blockIdx.x == 0 && blockIdx.y == 0 && tid == 0)
-      B.cmax_clear[0] = B.cmax_clear[1] = B.cmax_clear[2] = 0ull;
-  }
-  __syncthreads();
-
-  const int lxo = tx + HALO, lyo = ty + HALO;
-  const int gi = T.x0 + tx, gj = T.y0 + ty;
-  const bool active = gi <= n0 - 3 && gj <= n1 - 3;
-  const int gidx[2] = {gi, gj};
-  const int nn[2] = {n0, n1};
-
-  double out[6];
-#pragma unroll
-  for (int f = 0; f < 6; f++) out[f] = (MODE == SMAUG_INT_EULER) ? T.s(f, lxo, lyo) : 0.0;
-
-  // velocities for the background coupling terms (computevel3)
-  if (P.has_bg) {
-    for (int r = tid; r < RC; r += NTHREADS) {
-      int lx = r % RX, ly = r / RX;
-      double rt = T.S[RHO * RC + r] + T.S[RHOB * RC + r];
-      T.X[5 * RC + r] = T.S[M1 * RC + r] / rt;
-      T.X[6 * RC + r] = T.S[M2 * RC + r] / rt;
-      (void)lx; (void)ly;
-    }
-  }
-
-  // ---- fluxes and divergence, per direction (centdiff1 / centdiff2) ------
-  for (int d = 0; d < 2; d++) {
-    // flux region: halo 2 along d, tile extent across
-    const int ex = (d == 0) ? TX + 4 : TX, ey = (d == 0) ? TY : TY + 4;
-    const int ox = (d == 0) ? 1 : HALO, oy = (d == 0) ? HALO : 1;
-    for (int r = tid; r < ex * ey; r += NTHREADS) {
-      int lx = ox + r % ex, ly = oy + r / ex;
-      int ci = T.x0 - HALO + lx, cj = T.y0 - HALO + ly;
-      double F[5] = {0, 0, 0, 0, 0};
-      if (ci >= 0 && ci < n0 && cj >= 0 && cj < n1) {
-        double v[NF2];
-        load_cell(T, lx, ly, v);
-        fluxes2(P.gamma, v, d, F);
-      }
-#pragma unroll
-      for (int k = 0; k < 5; k++) T.x(k, lx, ly) = F[k];
-    }
-    __syncthreads();
-    if (active) {
-      const int a = gidx[d], n = nn[d];
-      const int sx = (d == 0), sy = (d == 1);
-      const double dl = B.delx[d][a];
-      const bool z = (P.bt[d] != 0) && zero3dn(a, n);
-      const int fld[5] = {RHO, M1, M2, EN, (d == 0) ? B2 : B1};
-#pragma unroll
-      for (int k = 0; k < 5; k++) {
-        double fp1 = T.x(k, lxo + sx, lyo + sy), fm1 = T.x(k, lxo - sx, lyo - sy);
-        double fp2 = T.x(k, lxo + 2 * sx, lyo + 2 * sy), fm2 = T.x(k, lxo - 2 * sx, lyo - 2 * sy);
-        double g = ((8 * fp1 - 8 * fm1 + fm2 - fp2) / 6.0) / (2.0 * dl);
-        if (z) g = 0;
-        out[fld[k]] = out[fld[k]] - dt * g;
-        if (k == 3 && P.has_bg) {
-          // addenergyterms_cd2 (src/centdiff2.cu:80-115)
-          const double eb = T.s(EB, lxo, lyo), bb1 = T.s(BB1, lxo, lyo), bb2 = T.s(BB2, lxo, lyo);
-          const double ptb = (P.gamma - 1) * eb - 0.5 * (P.gamma - 2) * (bb1 * bb1 + bb2 * bb2);
-          const int vk = 5 + d;
-          double gv;
-          {
-            double a1 = T.x(vk, lxo + sx, lyo + sy), a_1 = T.x(vk, lxo - sx, lyo - sy);
-            double a2 = T.x(vk, lxo + 2 * sx, lyo + 2 * sy), a_2 = T.x(vk, lxo - 2 * sx, lyo - 2 * sy);
-            gv = ((8 * a1 - 8 * a_1 + a_2 - a2) / 6.0) / (2.0 * dl);
-            if (z) gv = 0;
-          }
-          out[EN] -= +(dt)*ptb * gv;
-          const double bbd = (d == 0) ? bb1 : bb2;
-#pragma unroll
-          for (int idim = 0; idim < 2; idim++) {
-            const int tx2 = (idim == 0), ty2 = (idim == 1);
-            const int ai = gidx[idim], ni = nn[idim];
-            double a1 = T.x(vk, lxo + tx2, lyo + ty2), a_1 = T.x(vk, lxo - tx2, lyo - ty2);
-            double a2 = T.x(vk, lxo + 2 * tx2, lyo + 2 * ty2), a_2 = T.x(vk, lxo - 2 * tx2, lyo - 2 * ty2);
-            double gi2 = ((8 * a1 - 8 * a_1 + a_2 - a2) / 6.0) / (2.0 * B.delx[idim][ai]);
-            if ((P.bt[idim] != 0) && zero3dn(ai, ni)) gi2 = 0;
-            const double bbi = (idim == 0) ? bb1 : bb2;
-            out[EN] += (dt)*bbi * bbd * gi2;
-          }
-        }
-      }
-    }
-    __syncthreads();
-  }
-
-  // ---- gravity (addgrav_cd2, src/centdiff2.cu:118-154) --------------------
-  if (P.has_grav && active) {
-    const double rho = T.s(RHO, lxo, lyo), rhob = T.s(RHOB, lxo, lyo);
-    out[M1] += (dt) * (P.g[0]) * rho;
-    out[M2] += (dt) * (P.g[1]) * rho;
-    out[EN] += (dt)*rho * ((P.g[0]) * T.s(M1, lxo, lyo)) / (rho + rhob);
-    out[EN] += (dt)*rho * ((P.g[1]) * T.s(M2, lxo, lyo)) / (rho + rhob);
-  }
-
-  // ---- hyperdiffusion ------------------------------------------------------
-  if (P.hyperdif == 1) {
-    // pass list in the driver's order (src/iosmaug.c:696-810):
-    // kind 0 rho, 1 energy, 2 momentum component, 3 B component
-    const int npass = 10;
-    const int pk[npass] = {0, 0, 1, 1, 2, 2, 2, 2, 3, 3};
-    const int pc[npass] = {0, 0, 0, 0, 0, 1, 0, 1, 1, 0};
-    const int pd[npass] = {0, 1, 0, 1, 0, 0, 1, 1, 0, 1};
-    for (int ip = 0; ip < npass; ip++) {
-      const int kind = pk[ip], comp = pc[ip], dim = pd[ip];
-      const int qfield = (kind == 0) ? RHO : (kind == 1) ? EN : (kind == 2) ? M1 + comp : B1 + comp;
-      const double coef = B.cmax_in[dim];
-      const double chyp = P.chyp[qfield];
-      const int sx = (dim == 0), sy = (dim == 1);
-      const int nd_ = nn[dim];
-      // (A) q over the tile, halo 3 along dim, 1 across
-      {
-        const int ex = (dim == 0) ? RX : TX + 2, ey = (dim == 0) ? TY + 2 : RY;
-        const int ox = (dim == 0) ? 0 : HALO - 1, oy = (dim == 0) ? HALO - 1 : 0;
-        for (int r = tid; r < ex * ey; r += NTHREADS) {
-          int lx = ox + r % ex, ly = oy + r / ex;
-          int ci = T.x0 - HALO + lx, cj = T.y0 - HALO + ly;
-          int a = (dim == 0) ? ci : cj, tr = (dim == 0) ? cj : ci, ntr = (dim == 0) ? n1 : n0;
-          double q = 0.0;
-          if (tr >= 0 && tr < ntr) {
-            if (a >= 0 && a < nd_) {
-              double v[NF2];
-              load_cell(T, lx, ly, v);
-              q = hq2(kind, comp, v);
-            } else if (a == -1) {
-              // left pad: bc_hyperdifl copies index 5 (src/hyperdifvisc1l.cu:30-44)
-              int l5x = (dim == 0) ? lx + 6 : lx, l5y = (dim == 0) ? ly : ly + 6;
-              double v[NF2];
-              load_cell(T, l5x, l5y, v);
-              q = hq2(kind, comp, v);
-            } else if (a == nd_) {
-              // right pad: stray tmp6 store of hyperdifvisc1r_parallel
-              int src = B.padsrc[dim][tr];
-              if (src >= 0) {
-                double v[NF2];
-#pragma unroll
-                for (int f = 0; f < 6; f++) v[f] = B.uin[f * nc + src];
-#pragma unroll
-                for (int f = 0; f < 4; f++) v[6 + f] = B.bg[f * nc + src];
-                q = hq2(kind, comp, v);
-              }
-            }
-          }
-          T.x(0, lx, ly) = q;
-        }
-      }
-      __syncthreads();
-      // (B) nu_r, nu_l on the tile and one cell across (hyperdifvisc2-4)
-      {
-        const int ex = (dim == 0) ? TX : TX + 2, ey = (dim == 0) ? TY + 2 : TY;
-        const int ox = (dim == 0) ? HALO : HALO - 1, oy = (dim == 0) ? HALO - 1 : HALO;
-        for (int r = tid; r < ex * ey; r += NTHREADS) {
-          int lx = ox + r % ex, ly = oy + r / ex;
-          int ci = T.x0 - HALO + lx, cj = T.y0 - HALO + ly;
-          double nur = 0.0, nul = 0.0;
-          if (ci >= 2 && ci <= n0 - 3 && cj >= 2 && cj <= n1 - 3) {
-            double q[8];  // q(a-3 .. a+4)
-#pragma unroll
-            for (int s = 0; s < 7; s++) q[s] = T.x(0, lx + (s - 3) * sx, ly + (s - 3) * sy);
-            q[7] = 0.0;
-            // faces f+1/2, f = a-3 .. a+2 ; D3 needs f-1..f+2
-            double d1[6], d3[4];
-#pragma unroll
-            for (int k = 0; k < 6; k++) d1[k] = fabs(q[k + 1] - q[k]);          // f = a-3+k
-#pragma unroll
-            for (int k = 0; k < 4; k++)                                        // f = a-2+k
-              d3[k] = fabs(3.0 * (q[k + 2] - q[k + 1]) - (q[k + 3] - q[k]));
-            double t4r = 0, t5r = 0, t4l = 0, t5l = 0;
-            t4r = dmax0(t4r, d3[1]); t4r = dmax0(t4r, d3[2]); t4r = dmax0(t4r, d3[3]);
-            t4l = dmax0(t4l, d3[0]); t4l = dmax0(t4l, d3[1]); t4l = dmax0(t4l, d3[2]);
-#pragma unroll
-            for (int k = 1; k < 6; k++) t5r = dmax0(t5r, d1[k]);
-#pragma unroll
-            for (int k = 0; k < 5; k++) t5l = dmax0(t5l, d1[k]);
-            const int a = (dim == 0) ? ci : cj;
-            const double dl = B.delx[dim][a];
-            if (t5r > 0) nur = dl * (coef) * (chyp) * t4r / t5r;
-            if (t5l > 0) nul = dl * (coef) * (chyp) * t4l / t5l;
-          }
-          T.x(1, lx, ly) = nur;
-          T.x(2, lx, ly) = nul;
-        }
-      }
-      __syncthreads();
-      // (C) cross-term arrays on the tile and one cell across
-      const bool cross = (kind == 2 && comp != dim) || (kind == 3);
-      if (cross) {
-        const int ex = (dim == 0) ? TX : TX + 2, ey = (dim == 0) ? TY + 2 : TY;
-        const int ox = (dim == 0) ? HALO : HALO - 1, oy = (dim == 0) ? HALO - 1 : HALO;
-        for (int r = tid; r < ex * ey; r += NTHREADS) {
-          int lx = ox + r % ex, ly = oy + r / ex;
-          int ci = T.x0 - HALO + lx, cj = T.y0 - HALO + ly;
-          double c3 = 0.0, c4 = 0.0;
-          if (ci >= 0 && ci < n0 && cj >= 0 && cj < n1) {
-            const int a = (dim == 0) ? ci : cj;
-            double g = 0.0;
-            if (ci > 0 && ci < n0 - 1 && cj > 0 && cj < n1 - 1) {
-              // grad13n (src/gradops.cu:755-823)
-              g = ((T.x(0, lx + sx, ly + sy) - T.x(0, lx - sx, ly - sy)) / (B.delx[dim][a])) / 2.0;
-              if ((P.bt[dim] != 0) && zero1n(a, nd_)) g = 0;
-            }
-            const double nur = T.x(1, lx, ly), nul = T.x(2, lx, ly);
-            if (kind == 2) {
-              // hyperdifmomsourcene2-4 (src/hyperdifmomsourcene1.cu:325-565)
-              double tau = g * ((nur + nul + 2.0 * 0.0)) / 4.0;
-              c3 = (T.s(RHO, lx, ly) + T.s(RHOB, lx, ly)) * tau;
-              c4 = tau * T.s(M1 + dim, lx, ly);
-            } else {
-              // hyperdifbsourcene1b-4 (src/hyperdifbsourcene1.cu:290-598)
-              double t3 = g * (nul + nur) / 2;
-              c3 = t3;
-              c4 = t3 * T.s(B1 + dim, lx, ly);
-            }
-          }
-          T.x(3, lx, ly) = c3;
-          T.x(4, lx, ly) = c4;
-        }
-        __syncthreads();
-      }
-      // (D) apply the sources at the tile cells
-      if (active) {
-        const int a = gidx[dim];
-        const double dl = B.delx[dim][a];
-        const double rdx = dl;
-        const double nur = T.x(1, lxo, lyo), nul = T.x(2, lxo, lyo);
-        const double q0 = T.x(0, lxo, lyo), qp = T.x(0, lxo + sx, lyo + sy), qm = T.x(0, lxo - sx, lyo - sy);
-        const bool z1 = (P.bt[dim] != 0) && zero1n(a, nd_);
-        double gr = (qp - q0) / (dl);   // grad1r3n
-        double gl = (q0 - qm) / (dl);   // grad1l3n
-        if (z1) { gr = 0; gl = 0; }
-        if (kind == 0) {
-          out[RHO] = out[RHO] + dt * ((nur + 0.0) * gr - (nul + 0.0) * gl) / rdx;
-        } else if (kind == 1) {
-          out[EN] = out[EN] + dt * ((nur + 0.0) * gr - (nul + 0.0) * gl) / rdx;
-        } else if (kind == 2) {
-          // hyperdifmomsource1-3a (src/hyperdifmomsource1.cu:17-511), ii0 = comp
-          const double r0 = T.s(RHO, lxo, lyo), rb0 = T.s(RHOB, lxo, lyo);
-          const double t2 = (r0 + rb0 + T.s(RHO, lxo - sx, lyo - sy) + T.s(RHOB, lxo - sx, lyo - sy)) / 2;
-          const double t3 = (r0 + rb0 + T.s(RHO, lxo + sx, lyo + sy) + T.s(RHOB, lxo + sx, lyo + sy)) / 2;
-          const double mf = T.s(M1 + comp, lxo, lyo);
-          const double t5 = (mf + T.s(M1 + comp, lxo - sx, lyo - sy)) / 2;
-          const double t6 = (mf + T.s(M1 + comp, lxo + sx, lyo + sy)) / 2;
-          const double dm = (t3 * (nur + 0.0) * gr - t2 * (nul + 0.0) * gl) / (rdx) / 2;
-          const double de = (t6 * (nur + 0.0) * gr - t5 * (nul + 0.0) * gl) / (rdx) / 2;
-          out[M1 + comp] = out[M1 + comp] + dt * dm;
-          out[EN] = out[EN] + dt * de;
-          if (comp == dim) {
-            out[M1 + comp] = out[M1 + comp] + dt * dm;
-            out[EN] = out[EN] + dt * de;
-          } else {
-            // hyperdifmomsourcene5-6a: d/dx_comp of (rho_t tau) and (tau m_dim)
-            const int f = comp, fx = (f == 0), fy = (f == 1);
-            const int af = gidx[f];
-            const double dlf = B.delx[f][af];
-            double g7 = ((T.x(3, lxo + fx, lyo + fy) - T.x(3, lxo - fx, lyo - fy)) / (dlf)) / 2.0;
-            double g8 = ((T.x(4, lxo + fx, lyo + fy) - T.x(4, lxo - fx, lyo - fy)) / (dlf)) / 2.0;
-            if ((P.bt[f] != 0) && zero1n(af, nn[f])) { g7 = 0; g8 = 0; }
-            out[M1 + dim] = out[M1 + dim] + dt * g7;
-            out[EN] = out[EN] + dt * g8;
-          }
-        } else {
-          // B component comp, diffused along dim != comp
-          // hyperdifbsourcene (jj=dim, ii0=dim, mm=comp, sb=-1)
-          const int f = comp, fx = (f == 0), fy = (f == 1);
-          const int af = gidx[f];
-          const double dlf = B.delx[f][af];
-          double g4 = ((T.x(3, lxo + fx, lyo + fy) - T.x(3, lxo - fx, lyo - fy)) / (dlf)) / 2.0;
-          double g6 = ((T.x(4, lxo + fx, lyo + fy) - T.x(4, lxo - fx, lyo - fy)) / (dlf)) / 2.0;
-          if ((P.bt[f] != 0) && zero1n(af, nn[f])) { g4 = 0; g6 = 0; }
-          out[B1 + dim] = out[B1 + dim] + dt * (-1.0 * g4);
-          out[EN] = out[EN] + dt * (-1.0 * g6);
-          // hyperdifbsource (jj=comp, ii0=comp, mm=dim, sb=+1)
-          const double t2 = (q0 + qm) / 2, t3 = (q0 + qp) / 2;
-          const double dB = 1.0 * (gr * nur - gl * nul) / rdx;
-          const double de = 1.0 * (t3 * gr * nur - t2 * gl * nul) / rdx;
-          out[B1 + comp] = out[B1 + comp] + dt * dB;
-          out[EN] = out[EN] + dt * de;
-        }
-      }
-      __syncthreads();
-    }
-  }
-
-  // ---- user driver (source_parallel + addsourceterms2) ---------------------
-  if (P.driver == SMAUG_DRIVER_GAUSS && active) {
-    double v = P.drv_amp;
-    if (P.drv_period > 0) v *= sin(tstage * 2.0 * M_PI / P.drv_period);
-    for (int d = 0; d < 2; d++) {
-      if (P.drv_sigma[d] > 0) {
-        double x = B.pos[d][gidx[d]] - P.drv_x0[d];
-        v *= exp(-x * x / (P.drv_sigma[d] * P.drv_sigma[d]));
-      }
-    }
-    const double rr = (MODE == SMAUG_INT_EULER) ? out[RHO] : T.s(RHO, lxo, lyo);
-    out[M1] = out[M1] + (dt)*v * (rr + T.s(RHOB, lxo, lyo));
-  }
-
-  // ---- combine, write, ghost images, CFL maxima -----------------------------
-  double cm[2] = {0.0, 0.0};
-  if (active) {
-    double res[6];
-    const long c = (long)gj * n0 + gi;
-    if (MODE == SMAUG_INT_EULER) {
-#pragma unroll
-      for (int f = 0; f < 6; f++) res[f] = out[f];
-    } else {
-      const double wgt = (B.stage == 0 || B.stage == 3) ? 1.0 / 6.0 : 1.0 / 3.0;
-      const double cst = (B.stage == 2) ? 1.0 : 0.5;
-#pragma unroll
-      for (int f = 0; f < 6; f++) {
-        const double dl = out[f];
-        if (B.stage == 0) {
-          const double u = T.s(f, lxo, lyo);
-          B.acc[f * nc + c] = u + wgt * dl;
-          res[f] = u + cst * dl;
-        } else if (B.stage < 3) {
-          B.acc[f * nc + c] = B.acc[f * nc + c] + wgt * dl;
-          res[f] = B.un[f * nc + c] + cst * dl;
-        } else {
-          res[f] = B.acc[f * nc + c] + wgt * dl;
-        }
-      }
-    }
-    bool bad = false;
-#pragma unroll
-    for (int f = 0; f < 6; f++) bad |= !isfinite(res[f]);
-    if (bad) atomicOr(B.flags, 1);
-    int ix[3], iy[3];
-    ix[0] = gi;
-    iy[0] = gj;
-    int nx = 1 + ghost_images(gi, n0, P.bc[0], ix + 1);
-    int ny = 1 + ghost_images(gj, n1, P.bc[1], iy + 1);
-    for (int b = 0; b < ny; b++)
-      for (int a = 0; a < nx; a++) {
-        const long cc = (long)iy[b] * n0 + ix[a];
-#pragma unroll
-        for (int f = 0; f < 6; f++) B.uout[f * nc + cc] = res[f];
-        double eb, rb, b1b, b2b;
-        if (a == 0 && b == 0) {
-          eb = T.s(EB, lxo, lyo); rb = T.s(RHOB, lxo, lyo); b1b = T.s(BB1, lxo, lyo); b2b = T.s(BB2, lxo, lyo);
-        } else {
-          eb = B.bg[0 * nc + cc]; rb = B.bg[1 * nc + cc]; b1b = B.bg[2 * nc + cc]; b2b = B.bg[3 * nc + cc];
-        }
-#pragma unroll
-        for (int d = 0; d < 2; d++) {
-          double cf = cfast2(P.gamma, res[RHO], res[M1], res[M2], res[EN], res[B1], res[B2], eb, rb, b1b,
-                             b2b, d);
-          cm[d] = dmax0(cm[d], cf);
-        }
-      }
-  }
-  // block max -> atomicMax (non-negative doubles order like their bit patterns)
-  __shared__ double red[NTHREADS / 32][2];
-#pragma unroll
-  for (int d = 0; d < 2; d++) {
-    double v = cm[d];
-    for (int o = 16; o > 0; o >>= 1) v = dmax0(v, __shfl_xor_sync(0xffffffffu, v, o));
-    if ((tid & 31) == 0) red[tid >> 5][d] = v;
-  }
-  __syncthreads();
-  if (tid < 2) {
-    double v = 0.0;
-    for (int w = 0; w < NTHREADS / 32; w++) v = dmax0(v, red[w][tid]);
-    atomicMax(&B.cmax_out[tid], (unsigned long long)__double_as_longlong(v));
-  }
-}
+#include "stage2d.cuh"
 
 // ---------------------------------------------------------------------------
 // auxiliary kernels: ghost fill and CFL maxima of an arbitrary state
@@ -889,10 +410,9 @@ static int create(const smaug_params_t* p, const double* w, const double* pos, E
   K.has_grav = 0;
   for (int d = 0; d < e->nd; d++) if (p->g[d] != 0.0) K.has_grav = 1;
   K.has_bg = 0;
-  for (int f = 2 + 2 * e->nd; f < nvar; f++)
-    if (f != 3 + 2 * e->nd)  // rhob does not enter the coupling terms
-      for (long c = 0; c < nc; c++)
-        if (w[(size_t)f * nc + c] != 0.0) { K.has_bg = 1; break; }
+  for (int f = 2 + 2 * e->nd; f < nvar && !K.has_bg; f++)
+    for (long c = 0; c < nc; c++)
+      if (w[(size_t)f * nc + c] != 0.0) { K.has_bg = 1; break; }
   K.driver = p->driver;
   K.drv_amp = p->drv_amp;
   K.drv_period = p->drv_period;
@@ -934,10 +454,7 @@ static int create(const smaug_params_t* p, const double* w, const double* pos, E
   E_TRY(cudaMemcpy(e->d_dt, dt0, sizeof(dt0), cudaMemcpyHostToDevice));
   E_TRY(cudaMemcpy(e->d_t, t0, sizeof(t0), cudaMemcpyHostToDevice));
   E_TRY(cudaMemset(e->d_flags, 0, sizeof(int)));
-  E_TRY(cudaFuncSetAttribute(stage2d_kernel<SMAUG_INT_EULER>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM2D));
-  E_TRY(cudaFuncSetAttribute(stage2d_kernel<SMAUG_INT_RK4>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM2D));
+  E_TRY(stage2d_set_attributes());
 #undef E_TRY
   *out = e;
   return SMAUG_OK;
@@ -979,13 +496,10 @@ static int launch_stage(Engine* e, int mode, int stage, const double* uin, const
   B.flags = e->d_flags;
   B.mode = mode;
   B.stage = stage;
-  dim3 block(TX, TY);
-  dim3 grid((e->K.n0 - 4 + TX - 1) / TX, (e->K.n1 - 4 + TY - 1) / TY);
   if (mode == SMAUG_INT_EULER)
-    stage2d_kernel<SMAUG_INT_EULER><<<grid, block, SMEM2D, e->stream>>>(e->K, B);
+    CUDA_TRY(launch_stage2d<SMAUG_INT_EULER>(e->K, B, e->stream));
   else
-    stage2d_kernel<SMAUG_INT_RK4><<<grid, block, SMEM2D, e->stream>>>(e->K, B);
-  CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(launch_stage2d<SMAUG_INT_RK4>(e->K, B, e->stream));
   e->stage_count++;
   return SMAUG_OK;
 }
@@ -1325,12 +839,8 @@ extern "C" int smaug_euler_step_noalloc(const smaug_params_t* p, const double* w
   B.flags = flags;
   B.mode = SMAUG_INT_EULER;
   B.stage = 0;
-  CUDA_TRY(cudaFuncSetAttribute(stage2d_kernel<SMAUG_INT_EULER>,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM2D));
-  dim3 block(TX, TY);
-  dim3 grid((p->n[0] - 4 + TX - 1) / TX, (p->n[1] - 4 + TY - 1) / TY);
-  stage2d_kernel<SMAUG_INT_EULER><<<grid, block, SMEM2D, st>>>(K, B);
-  CUDA_TRY(cudaGetLastError());
+  CUDA_TRY(stage2d_set_attributes());
+  CUDA_TRY(launch_stage2d<SMAUG_INT_EULER>(K, B, st));
   // background fields are constant: carry them to the output
   CUDA_TRY(cudaMemcpyAsync(w_out + 6 * nc, bg, sizeof(double) * 4 * nc, cudaMemcpyDeviceToDevice, st));
   int hflags = 0;

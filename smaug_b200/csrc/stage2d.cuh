@@ -1,0 +1,579 @@
+// stage2d.cuh -- fused 2D stage kernel (FP64), included by engine.cu.
+//
+// One launch evaluates the reference's whole spatial operator for a 32x8
+// tile of interior cells and writes the stage result, its ghost images and
+// the per-dimension fast-speed maxima.  Term by term it follows the launch
+// order of the reference's step (src/iosmaug.c:631-835); the arithmetic of
+// each term is the reference's, with divisions by rho_t and by the cell
+// width replaced by multiplications with per-cell / per-line reciprocals
+// (agreement with the reference stays at rounding level, ~1e-16 relative).
+//
+// Shared memory (doubles): NS state fields x RC, 1/rho_t x RC, the tile's
+// cell widths and their reciprocals, then one union of phase scratch:
+//   flux phase:  5 flux arrays on the tile +-2 cells along the direction
+//                (+ 2 velocity arrays when background fields are present)
+//   hyperdiffusion phase: q on the tile +-3 along dim / +-1 across,
+//                nu_r, nu_l and two cross-term arrays on the tile +-1 across.
+#pragma once
+
+// (included inside namespace smaug)
+namespace s2 {
+constexpr int FSZ = (TX + 4) * TY > TX * (TY + 4) ? (TX + 4) * TY : TX * (TY + 4);
+constexpr int QSZ = RX * (TY + 2) > (TX + 2) * RY ? RX * (TY + 2) : (TX + 2) * RY;
+constexpr int NSZ = TX * (TY + 2) > (TX + 2) * TY ? TX * (TY + 2) : (TX + 2) * TY;
+constexpr int FLUX_SCR = 5 * FSZ;
+constexpr int HYP_SCR = QSZ + 4 * NSZ;
+constexpr int UNION = FLUX_SCR > HYP_SCR ? FLUX_SCR : HYP_SCR;
+template <bool BG>
+__host__ __device__ constexpr int nstate() { return BG ? 10 : 6; }
+template <bool BG>
+__host__ __device__ constexpr size_t smem_bytes() {
+  return sizeof(double) * ((size_t)(nstate<BG>() + 1 + (BG ? 2 : 0)) * RC + 2 * (RX + RY) + UNION);
+}
+}  // namespace s2
+
+template <bool BG>
+struct T2 {
+  double* S;     // [NS][RC] state
+  double* R;     // [RC] 1/rho_t
+  double* V;     // [2][RC] velocities (BG only)
+  double* dl0;   // [RX] widths along x of the region columns
+  double* dl1;   // [RY]
+  double* rd0;   // [RX] reciprocals
+  double* rd1;   // [RY]
+  double* U;     // union scratch
+  int x0, y0;
+  __device__ __forceinline__ double s(int f, int l) const {
+    if (BG) return S[f * RC + l];
+    return (f < 6) ? S[f * RC + l] : (f == RHOB ? 0.0 : 0.0);
+  }
+};
+
+// fluxes along D of rho, m1, m2, e and the B component across D at region
+// cell l (src/centdiff1.cu:51-197, src/centdiff2.cu:203-323):
+//   F_rho = m_D (= m_D rho'/rho_t + rho_b m_D/rho_t)
+//   F_m_c = v_D m_c + delta_cD p_t - (B'_c Bb_D + Bb_c B'_D) - B'_c B'_D
+//   F_e   = v_D (e + p_t + e_b) - (B'_D (Bb.m) + Bb_D (B'.m) + B'_D (B'.m)) / rho_t
+//   F_B_c = v_D (B'_c + Bb_c) - v_c (B'_D + Bb_D)
+template <bool BG, int D>
+__device__ __forceinline__ void flux_at(const T2<BG>& T, double gamma, int l, double* F) {
+  const double rho = T.S[RHO * RC + l], m1 = T.S[M1 * RC + l], m2 = T.S[M2 * RC + l];
+  const double e = T.S[EN * RC + l], b1 = T.S[B1 * RC + l], b2 = T.S[B2 * RC + l];
+  double eb = 0, bb1 = 0, bb2 = 0;
+  if (BG) {
+    eb = T.S[EB * RC + l];
+    bb1 = T.S[BB1 * RC + l];
+    bb2 = T.S[BB2 * RC + l];
+  }
+  const double r = T.R[l];
+  const double md = D == 0 ? m1 : m2;
+  const double vd = md * r;
+  // computept3 (src/dervfields.cu:107-153)
+  const double pt = (gamma - 1.0) * (e - 0.5 * (m1 * m1 + m2 * m2) * r) -
+                    (gamma - 2.0) * ((b1 * bb1 + b2 * bb2) + 0.5 * (b1 * b1 + b2 * b2));
+  const double bd = D == 0 ? b1 : b2, bbd = D == 0 ? bb1 : bb2;
+  F[0] = md;
+  // momentum components
+  F[1] = vd * m1 + (D == 0 ? pt : 0.0) - (b1 * bbd + bb1 * bd) - b1 * bd;
+  F[2] = vd * m2 + (D == 1 ? pt : 0.0) - (b2 * bbd + bb2 * bd) - b2 * bd;
+  // energy
+  const double bbm = bb1 * m1 + bb2 * m2, bm = b1 * m1 + b2 * m2;
+  F[3] = vd * (e + pt + eb) - (bd * bbm + bbd * bm + bd * bm) * r;
+  // B component across D
+  if (D == 0)
+    F[4] = vd * (b2 + bb2) - (m2 * r) * (b1 + bb1);
+  else
+    F[4] = vd * (b1 + bb1) - (m1 * r) * (b2 + bb2);
+}
+
+// 4th-order centred derivative along the stride s (grad3dn, src/gradops.cu:437-602)
+__device__ __forceinline__ double d4(const double* a, int l, int s, double rdl2) {
+  return ((8.0 * (a[l + s] - a[l - s]) + (a[l - 2 * s] - a[l + 2 * s])) * (1.0 / 6.0)) * rdl2;
+}
+
+// q of a hyperdiffusion pass at region cell l (src/hyperdifvisc1r.cu:1225-1253)
+template <bool BG, int KIND, int COMP>
+__device__ __forceinline__ double hq_at(const T2<BG>& T, int l) {
+  if (KIND == 0) return T.S[RHO * RC + l];
+  if (KIND == 1) {
+    const double m1 = T.S[M1 * RC + l], m2 = T.S[M2 * RC + l];
+    const double b1 = T.S[B1 * RC + l], b2 = T.S[B2 * RC + l];
+    return T.S[EN * RC + l] - 0.5 * ((b1 * b1 + b2 * b2) + (m1 * m1 + m2 * m2) * T.R[l]);
+  }
+  if (KIND == 2) return T.S[(M1 + COMP) * RC + l] * T.R[l];
+  return T.S[(B1 + COMP) * RC + l];
+}
+
+// the same q from global memory (stray pad source cell)
+template <int KIND, int COMP>
+__device__ __forceinline__ double hq_global(const KBufs& B, long nc, long c) {
+  const double rho = B.uin[0 * nc + c], rhob = B.bg[1 * nc + c];
+  if (KIND == 0) return rho;
+  const double r = 1.0 / (rho + rhob);
+  if (KIND == 1) {
+    const double m1 = B.uin[1 * nc + c], m2 = B.uin[2 * nc + c];
+    const double b1 = B.uin[4 * nc + c], b2 = B.uin[5 * nc + c];
+    return B.uin[3 * nc + c] - 0.5 * ((b1 * b1 + b2 * b2) + (m1 * m1 + m2 * m2) * r);
+  }
+  if (KIND == 2) return B.uin[(1 + COMP) * nc + c] * r;
+  return B.uin[(4 + COMP) * nc + c];
+}
+
+// One hyperdiffusion pass: field kind (0 rho, 1 energy, 2 momentum, 3 B),
+// component COMP, direction DIM (src/iosmaug.c:696-810 order).
+template <bool BG, int KIND, int COMP, int DIM>
+__device__ __forceinline__ void hyper_pass(const T2<BG>& T, const KParams& P, const KBufs& B,
+                                           int tid, bool active, int lxo, int lyo, int gi, int gj,
+                                           double dt, double* out) {
+  constexpr int SX = (DIM == 0), SY = (DIM == 1);
+  constexpr int QFIELD = (KIND == 0) ? RHO : (KIND == 1) ? EN : (KIND == 2) ? M1 + COMP : B1 + COMP;
+  constexpr bool CROSS = (KIND == 2 && COMP != DIM) || (KIND == 3);
+  const int n0 = P.n0, n1 = P.n1;
+  const int nd = DIM == 0 ? n0 : n1;
+  const long nc = P.ncell;
+  double* Q = T.U;                  // region-indexed (RX stride) q
+  double* NR = T.U + s2::QSZ;       // nu_r, region-indexed rows/cols of the nu area
+  double* NL = NR + s2::NSZ;
+  double* C3 = NL + s2::NSZ;
+  double* C4 = C3 + s2::NSZ;
+  // nu area: tile along DIM, +-1 across; indexed (ly - oyN) * exN + (lx - oxN)
+  constexpr int exN = (DIM == 0) ? TX : TX + 2, eyN = (DIM == 0) ? TY + 2 : TY;
+  constexpr int oxN = (DIM == 0) ? HALO : HALO - 1, oyN = (DIM == 0) ? HALO - 1 : HALO;
+  // q area: full region along DIM, +-1 across; stored with region stride at region coords
+  constexpr int exQ = (DIM == 0) ? RX : TX + 2, eyQ = (DIM == 0) ? TY + 2 : RY;
+  constexpr int oxQ = (DIM == 0) ? 0 : HALO - 1, oyQ = (DIM == 0) ? HALO - 1 : 0;
+  // Q is stored in a compact array with row stride exQ
+  auto qi = [&](int lx, int ly) { return (ly - oyQ) * exQ + (lx - oxQ); };
+  auto ni = [&](int lx, int ly) { return (ly - oyN) * exN + (lx - oxN); };
+
+  // (A) q with the reference's pads at index -1 (copy of index 5,
+  // bc_hyperdifl) and index n (stray tmp6 store of hyperdifvisc1r_parallel)
+  for (int r = tid; r < exQ * eyQ; r += NTHREADS) {
+    const int lx = oxQ + r % exQ, ly = oyQ + r / exQ;
+    const int ci = T.x0 - HALO + lx, cj = T.y0 - HALO + ly;
+    const int a = DIM == 0 ? ci : cj, tr = DIM == 0 ? cj : ci, ntr = DIM == 0 ? n1 : n0;
+    double q = 0.0;
+    if (tr >= 0 && tr < ntr) {
+      if (a >= 0 && a < nd) {
+        q = hq_at<BG, KIND, COMP>(T, ly * RX + lx);
+      } else if (a == -1) {
+        q = hq_at<BG, KIND, COMP>(T, (ly + 6 * SY) * RX + lx + 6 * SX);
+      } else if (a == nd) {
+        const int src = B.padsrc[DIM][tr];
+        if (src >= 0) q = hq_global<KIND, COMP>(B, nc, src);
+      }
+    }
+    Q[r] = q;
+  }
+  __syncthreads();
+  // (B) nu_r, nu_l (hyperdifvisc2-4): third differences D3 over faces
+  // i-2..i+1, first differences D1 over faces i-3..i+2
+  const double coef = B.cmax_in[DIM] * P.chyp[QFIELD];
+  for (int r = tid; r < exN * eyN; r += NTHREADS) {
+    const int lx = oxN + r % exN, ly = oyN + r / exN;
+    const int ci = T.x0 - HALO + lx, cj = T.y0 - HALO + ly;
+    double nur = 0.0, nul = 0.0;
+    if (ci >= 2 && ci <= n0 - 3 && cj >= 2 && cj <= n1 - 3) {
+      const int q0 = qi(lx, ly);
+      constexpr int st = DIM == 0 ? 1 : exQ;
+      double q[7];
+#pragma unroll
+      for (int s = 0; s < 7; s++) q[s] = Q[q0 + (s - 3) * st];
+      double d1[6], d3[4];
+#pragma unroll
+      for (int k = 0; k < 6; k++) d1[k] = fabs(q[k + 1] - q[k]);
+#pragma unroll
+      for (int k = 0; k < 4; k++) d3[k] = fabs(3.0 * (q[k + 2] - q[k + 1]) - (q[k + 3] - q[k]));
+      double t4r = 0, t5r = 0, t4l = 0, t5l = 0;
+      t4r = dmax0(dmax0(dmax0(t4r, d3[1]), d3[2]), d3[3]);
+      t4l = dmax0(dmax0(dmax0(t4l, d3[0]), d3[1]), d3[2]);
+#pragma unroll
+      for (int k = 1; k < 6; k++) t5r = dmax0(t5r, d1[k]);
+#pragma unroll
+      for (int k = 0; k < 5; k++) t5l = dmax0(t5l, d1[k]);
+      const double c = (DIM == 0 ? T.dl0[lx] : T.dl1[ly]) * coef;
+      if (t5r > 0) nur = c * t4r / t5r;
+      if (t5l > 0) nul = c * t4l / t5l;
+    }
+    NR[r] = nur;
+    NL[r] = nul;
+  }
+  __syncthreads();
+  // (C) cross-term arrays (hyperdifmomsourcene2-4 / hyperdifbsourcene1b-4)
+  if (CROSS) {
+    for (int r = tid; r < exN * eyN; r += NTHREADS) {
+      const int lx = oxN + r % exN, ly = oyN + r / exN;
+      const int ci = T.x0 - HALO + lx, cj = T.y0 - HALO + ly;
+      double c3 = 0.0, c4 = 0.0;
+      if (ci > 0 && ci < n0 - 1 && cj > 0 && cj < n1 - 1) {
+        const int a = DIM == 0 ? ci : cj;
+        const int q0 = qi(lx, ly);
+        constexpr int st = DIM == 0 ? 1 : exQ;
+        // grad13n along DIM of q
+        double g = ((Q[q0 + st] - Q[q0 - st]) * (DIM == 0 ? T.rd0[lx] : T.rd1[ly])) * 0.5;
+        if ((P.bt[DIM] != 0) && zero1n(a, nd)) g = 0;
+        const double nsum = NR[r] + NL[r];
+        const int l = ly * RX + lx;
+        if (KIND == 2) {
+          const double tau = (g * nsum) * 0.25;
+          c3 = (T.S[RHO * RC + l] + (BG ? T.S[RHOB * RC + l] : 0.0)) * tau;
+          c4 = tau * T.S[(M1 + DIM) * RC + l];
+        } else {
+          const double t3 = (g * nsum) * 0.5;
+          c3 = t3;
+          c4 = t3 * T.S[(B1 + DIM) * RC + l];
+        }
+      }
+      C3[r] = c3;
+      C4[r] = c4;
+    }
+    __syncthreads();
+  }
+  // (D) sources at the tile cells
+  if (active) {
+    const int a = DIM == 0 ? gi : gj;
+    const int q0 = qi(lxo, lyo);
+    constexpr int st = DIM == 0 ? 1 : exQ;
+    const int nidx = ni(lxo, lyo);
+    const double nur = NR[nidx], nul = NL[nidx];
+    const double rdl = DIM == 0 ? T.rd0[lxo] : T.rd1[lyo];
+    const double qc = Q[q0], qp = Q[q0 + st], qm = Q[q0 - st];
+    double gr = (qp - qc) * rdl;   // grad1r3n
+    double gl = (qc - qm) * rdl;   // grad1l3n
+    if ((P.bt[DIM] != 0) && zero1n(a, nd)) { gr = 0; gl = 0; }
+    const int l = lyo * RX + lxo;
+    constexpr int SL = SX + SY * RX;  // region stride along DIM
+    if (KIND == 0) {
+      out[RHO] = out[RHO] + dt * (nur * gr - nul * gl) * rdl;
+    } else if (KIND == 1) {
+      out[EN] = out[EN] + dt * (nur * gr - nul * gl) * rdl;
+    } else if (KIND == 2) {
+      // hyperdifmomsource1-3a (src/hyperdifmomsource1.cu:17-511), ii0 = COMP
+      const double rb0 = BG ? T.S[RHOB * RC + l] : 0.0;
+      const double rbm = BG ? T.S[RHOB * RC + l - SL] : 0.0;
+      const double rbp = BG ? T.S[RHOB * RC + l + SL] : 0.0;
+      const double r0 = T.S[RHO * RC + l];
+      const double t2 = (r0 + rb0 + T.S[RHO * RC + l - SL] + rbm) * 0.5;
+      const double t3 = (r0 + rb0 + T.S[RHO * RC + l + SL] + rbp) * 0.5;
+      const double mf = T.S[(M1 + COMP) * RC + l];
+      const double t5 = (mf + T.S[(M1 + COMP) * RC + l - SL]) * 0.5;
+      const double t6 = (mf + T.S[(M1 + COMP) * RC + l + SL]) * 0.5;
+      const double dm = ((t3 * nur * gr - t2 * nul * gl) * rdl) * 0.5;
+      const double de = ((t6 * nur * gr - t5 * nul * gl) * rdl) * 0.5;
+      out[M1 + COMP] = out[M1 + COMP] + dt * dm;
+      out[EN] = out[EN] + dt * de;
+      if (COMP == DIM) {
+        out[M1 + COMP] = out[M1 + COMP] + dt * dm;
+        out[EN] = out[EN] + dt * de;
+      } else {
+        // hyperdifmomsourcene5-6a: d/dx_COMP of (rho_t tau) and (tau m_DIM)
+        constexpr int FS = (COMP == 0) ? 1 : exN;  // stride across in the nu area
+        const int af = COMP == 0 ? gi : gj;
+        const double rdf = COMP == 0 ? T.rd0[lxo] : T.rd1[lyo];
+        double g7 = ((C3[nidx + FS] - C3[nidx - FS]) * rdf) * 0.5;
+        double g8 = ((C4[nidx + FS] - C4[nidx - FS]) * rdf) * 0.5;
+        if ((P.bt[COMP] != 0) && zero1n(af, COMP == 0 ? n0 : n1)) { g7 = 0; g8 = 0; }
+        out[M1 + DIM] = out[M1 + DIM] + dt * g7;
+        out[EN] = out[EN] + dt * g8;
+      }
+    } else {
+      // B component COMP diffused along DIM: hyperdifbsourcene (sb=-1) then
+      // hyperdifbsource (sb=+1)
+      constexpr int FS = (COMP == 0) ? 1 : exN;
+      const int af = COMP == 0 ? gi : gj;
+      const double rdf = COMP == 0 ? T.rd0[lxo] : T.rd1[lyo];
+      double g4 = ((C3[nidx + FS] - C3[nidx - FS]) * rdf) * 0.5;
+      double g6 = ((C4[nidx + FS] - C4[nidx - FS]) * rdf) * 0.5;
+      if ((P.bt[COMP] != 0) && zero1n(af, COMP == 0 ? n0 : n1)) { g4 = 0; g6 = 0; }
+      out[B1 + DIM] = out[B1 + DIM] - dt * g4;
+      out[EN] = out[EN] - dt * g6;
+      const double t2 = (qc + qm) * 0.5, t3 = (qc + qp) * 0.5;
+      const double dB = (gr * nur - gl * nul) * rdl;
+      const double de = (t3 * gr * nur - t2 * gl * nul) * rdl;
+      out[B1 + COMP] = out[B1 + COMP] + dt * dB;
+      out[EN] = out[EN] + dt * de;
+    }
+  }
+  __syncthreads();
+}
+
+template <int MODE, bool BG>
+__global__ void __launch_bounds__(NTHREADS, 3) stage2d_fast(const KParams P, const KBufs B) {
+  extern __shared__ double smem[];
+  T2<BG> T;
+  constexpr int NS = s2::nstate<BG>();
+  T.S = smem;
+  T.R = smem + NS * RC;
+  T.V = T.R + RC;
+  T.dl0 = T.V + (BG ? 2 * RC : 0);
+  T.dl1 = T.dl0 + RX;
+  T.rd0 = T.dl1 + RY;
+  T.rd1 = T.rd0 + RX;
+  T.U = T.rd1 + RY;
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
+  T.x0 = 2 + blockIdx.x * TX;
+  T.y0 = 2 + blockIdx.y * TY;
+  const int n0 = P.n0, n1 = P.n1;
+  const long nc = P.ncell;
+
+  // ---- stage the tile, 1/rho_t, the metric -------------------------------
+  for (int r = tid; r < RC; r += NTHREADS) {
+    const int lx = r % RX, ly = r / RX;
+    const int gi = T.x0 - HALO + lx, gj = T.y0 - HALO + ly;
+    const bool in = gi >= 0 && gi < n0 && gj >= 0 && gj < n1;
+    const long c = (long)gj * n0 + gi;
+    double rho = 0.0, rhob = 1.0;
+#pragma unroll
+    for (int f = 0; f < 6; f++) {
+      const double v = in ? __ldg(B.uin + f * nc + c) : 0.0;
+      T.S[f * RC + r] = v;
+      if (f == 0) rho = v;
+    }
+    if (BG) {
+#pragma unroll
+      for (int f = 0; f < 4; f++) {
+        const double v = in ? __ldg(B.bg + f * nc + c) : (f == 1 ? 1.0 : 0.0);
+        T.S[(6 + f) * RC + r] = v;
+        if (f == 1) rhob = v;
+      }
+    } else {
+      rhob = in ? __ldg(B.bg + 1 * nc + c) : 1.0;
+      if (!in) rho = 0.0;
+    }
+    const double rinv = 1.0 / (rho + rhob);
+    T.R[r] = rinv;
+    if (BG) {
+      T.V[r] = T.S[M1 * RC + r] * rinv;
+      T.V[RC + r] = T.S[M2 * RC + r] * rinv;
+    }
+  }
+  for (int r = tid; r < RX + RY; r += NTHREADS) {
+    if (r < RX) {
+      const int gi = T.x0 - HALO + r;
+      const double d = (gi >= 0 && gi < n0) ? B.delx[0][gi] : 1.0;
+      T.dl0[r] = d;
+      T.rd0[r] = 1.0 / d;
+    } else {
+      const int gj = T.y0 - HALO + (r - RX);
+      const double d = (gj >= 0 && gj < n1) ? B.delx[1][gj] : 1.0;
+      T.dl1[r - RX] = d;
+      T.rd1[r - RX] = 1.0 / d;
+    }
+  }
+
+  // ---- dt of this step and stage time ----------------------------------
+  double dt, tstage;
+  if (B.stage == 0) {
+    dt = device_dt(P, B.cmax_in, *B.dt_prev, 2);
+    if (blockIdx.x == 0 && blockIdx.y == 0 && tid == 0) {
+      *B.dt_new = dt;
+      *B.t_new = *B.t_prev + dt;
+      B.cmax_clear[0] = B.cmax_clear[1] = B.cmax_clear[2] = 0ull;
+    }
+    tstage = *B.t_prev;
+  } else {
+    dt = *B.dt_new;
+    tstage = *B.t_prev + (B.stage == 3 ? dt : 0.5 * dt);
+    if (blockIdx.x == 0 && blockIdx.y == 0 && tid == 0)
+      B.cmax_clear[0] = B.cmax_clear[1] = B.cmax_clear[2] = 0ull;
+  }
+  __syncthreads();
+
+  const int lxo = tx + HALO, lyo = ty + HALO, lo = lyo * RX + lxo;
+  const int gi = T.x0 + tx, gj = T.y0 + ty;
+  const bool active = gi <= n0 - 3 && gj <= n1 - 3;
+
+  double out[6];
+#pragma unroll
+  for (int f = 0; f < 6; f++) out[f] = (MODE == SMAUG_INT_EULER) ? T.S[f * RC + lo] : 0.0;
+
+  // ---- fluxes and divergence (centdiff1 / centdiff2), direction 0 then 1 --
+#pragma unroll
+  for (int d = 0; d < 2; d++) {
+    const int ex = (d == 0) ? TX + 4 : TX, ey = (d == 0) ? TY : TY + 4;
+    const int ox = (d == 0) ? 1 : HALO, oy = (d == 0) ? HALO : 1;
+    double* F = T.U;
+    for (int r = tid; r < ex * ey; r += NTHREADS) {
+      const int lx = ox + r % ex, ly = oy + r / ex;
+      const int ci = T.x0 - HALO + lx, cj = T.y0 - HALO + ly;
+      double f5[5] = {0, 0, 0, 0, 0};
+      if (ci >= 0 && ci < n0 && cj >= 0 && cj < n1) {
+        if (d == 0)
+          flux_at<BG, 0>(T, P.gamma, ly * RX + lx, f5);
+        else
+          flux_at<BG, 1>(T, P.gamma, ly * RX + lx, f5);
+      }
+#pragma unroll
+      for (int k = 0; k < 5; k++) F[k * s2::FSZ + r] = f5[k];
+    }
+    __syncthreads();
+    if (active) {
+      const int a = d == 0 ? gi : gj, n = d == 0 ? n0 : n1;
+      const bool z = (P.bt[d] != 0) && zero3dn(a, n);
+      const double rdl2 = 0.5 * (d == 0 ? T.rd0[lxo] : T.rd1[lyo]);
+      const int fo = (lyo - oy) * ex + (lxo - ox);
+      const int fs = d == 0 ? 1 : ex;
+      const int fld[5] = {RHO, M1, M2, EN, d == 0 ? B2 : B1};
+#pragma unroll
+      for (int k = 0; k < 5; k++) {
+        double g = d4(F + k * s2::FSZ, fo, fs, rdl2);
+        if (z) g = 0;
+        out[fld[k]] = out[fld[k]] - dt * g;
+      }
+      if (BG) {
+        // addenergyterms_cd2 (src/centdiff2.cu:80-115)
+        const double eb = T.S[EB * RC + lo], bb1 = T.S[BB1 * RC + lo], bb2 = T.S[BB2 * RC + lo];
+        const double ptb = (P.gamma - 1) * eb - 0.5 * (P.gamma - 2) * (bb1 * bb1 + bb2 * bb2);
+        const double* v = T.V + d * RC;
+        double gv = d4(v, lo, d == 0 ? 1 : RX, rdl2);
+        if (z) gv = 0;
+        out[EN] -= dt * ptb * gv;
+        const double bbd = d == 0 ? bb1 : bb2;
+        double g0 = d4(v, lo, 1, 0.5 * T.rd0[lxo]);
+        if ((P.bt[0] != 0) && zero3dn(gi, n0)) g0 = 0;
+        out[EN] += dt * bb1 * bbd * g0;
+        double g1 = d4(v, lo, RX, 0.5 * T.rd1[lyo]);
+        if ((P.bt[1] != 0) && zero3dn(gj, n1)) g1 = 0;
+        out[EN] += dt * bb2 * bbd * g1;
+      }
+    }
+    __syncthreads();
+  }
+
+  // ---- gravity (addgrav_cd2, src/centdiff2.cu:118-154) --------------------
+  if (P.has_grav && active) {
+    const double rho = T.S[RHO * RC + lo];
+    out[M1] += dt * P.g[0] * rho;
+    out[M2] += dt * P.g[1] * rho;
+    const double rr = rho * T.R[lo];
+    out[EN] += (dt * P.g[0] * T.S[M1 * RC + lo]) * rr;
+    out[EN] += (dt * P.g[1] * T.S[M2 * RC + lo]) * rr;
+  }
+
+  // ---- hyperdiffusion, in the driver's order -------------------------------
+  if (P.hyperdif == 1) {
+    hyper_pass<BG, 0, 0, 0>(T, P, B, tid, active, lxo, lyo, gi, gj, dt, out);
+    hyper_pass<BG, 0, 0, 1>(T, P, B, tid, active, lxo, lyo, gi, gj, dt, out);
+    hyper_pass<BG, 1, 0, 0>(T, P, B, tid, active, lxo, lyo, gi, gj, dt, out);
+    hyper_pass<BG, 1, 0, 1>(T, P, B, tid, active, lxo, lyo, gi, gj, dt, out);
+    hyper_pass<BG, 2, 0, 0>(T, P, B, tid, active, lxo, lyo, gi, gj, dt, out);
+    hyper_pass<BG, 2, 1, 0>(T, P, B, tid, active, lxo, lyo, gi, gj, dt, out);
+    hyper_pass<BG, 2, 0, 1>(T, P, B, tid, active, lxo, lyo, gi, gj, dt, out);
+    hyper_pass<BG, 2, 1, 1>(T, P, B, tid, active, lxo, lyo, gi, gj, dt, out);
+    hyper_pass<BG, 3, 1, 0>(T, P, B, tid, active, lxo, lyo, gi, gj, dt, out);
+    hyper_pass<BG, 3, 0, 1>(T, P, B, tid, active, lxo, lyo, gi, gj, dt, out);
+  }
+
+  // ---- user driver (source_parallel + addsourceterms2) ---------------------
+  if (P.driver == SMAUG_DRIVER_GAUSS && active) {
+    double v = P.drv_amp;
+    if (P.drv_period > 0) v *= sin(tstage * 2.0 * M_PI / P.drv_period);
+    if (P.drv_sigma[0] > 0) {
+      const double x = B.pos[0][gi] - P.drv_x0[0];
+      v *= exp(-x * x / (P.drv_sigma[0] * P.drv_sigma[0]));
+    }
+    if (P.drv_sigma[1] > 0) {
+      const double x = B.pos[1][gj] - P.drv_x0[1];
+      v *= exp(-x * x / (P.drv_sigma[1] * P.drv_sigma[1]));
+    }
+    const double rhob = BG ? T.S[RHOB * RC + lo] : B.bg[1 * nc + (long)gj * n0 + gi];
+    const double rr = (MODE == SMAUG_INT_EULER) ? out[RHO] : T.S[RHO * RC + lo];
+    out[M1] = out[M1] + dt * v * (rr + rhob);
+  }
+
+  // ---- combine, write, ghost images, CFL maxima -----------------------------
+  double cm0 = 0.0, cm1 = 0.0;
+  if (active) {
+    double res[6];
+    const long c = (long)gj * n0 + gi;
+    if (MODE == SMAUG_INT_EULER) {
+#pragma unroll
+      for (int f = 0; f < 6; f++) res[f] = out[f];
+    } else {
+      const double wgt = (B.stage == 0 || B.stage == 3) ? 1.0 / 6.0 : 1.0 / 3.0;
+      const double cst = (B.stage == 2) ? 1.0 : 0.5;
+#pragma unroll
+      for (int f = 0; f < 6; f++) {
+        const double dl = out[f];
+        if (B.stage == 0) {
+          const double u = T.S[f * RC + lo];
+          B.acc[f * nc + c] = u + wgt * dl;
+          res[f] = u + cst * dl;
+        } else if (B.stage < 3) {
+          B.acc[f * nc + c] = B.acc[f * nc + c] + wgt * dl;
+          res[f] = B.un[f * nc + c] + cst * dl;
+        } else {
+          res[f] = B.acc[f * nc + c] + wgt * dl;
+        }
+      }
+    }
+    bool bad = false;
+#pragma unroll
+    for (int f = 0; f < 6; f++) bad |= !isfinite(res[f]);
+    if (bad) atomicOr(B.flags, 1);
+    int ix[3], iy[3];
+    ix[0] = gi;
+    iy[0] = gj;
+    const int nx = 1 + ghost_images(gi, n0, P.bc[0], ix + 1);
+    const int ny = 1 + ghost_images(gj, n1, P.bc[1], iy + 1);
+    for (int b = 0; b < ny; b++)
+      for (int a2 = 0; a2 < nx; a2++) {
+        const long cc = (long)iy[b] * n0 + ix[a2];
+#pragma unroll
+        for (int f = 0; f < 6; f++) B.uout[f * nc + cc] = res[f];
+        double eb, rb, b1b, b2b;
+        if (BG && a2 == 0 && b == 0) {
+          eb = T.S[EB * RC + lo]; rb = T.S[RHOB * RC + lo]; b1b = T.S[BB1 * RC + lo]; b2b = T.S[BB2 * RC + lo];
+        } else {
+          eb = B.bg[0 * nc + cc]; rb = B.bg[1 * nc + cc]; b1b = B.bg[2 * nc + cc]; b2b = B.bg[3 * nc + cc];
+        }
+        cm0 = dmax0(cm0, cfast2(P.gamma, res[RHO], res[M1], res[M2], res[EN], res[B1], res[B2], eb, rb,
+                                b1b, b2b, 0));
+        cm1 = dmax0(cm1, cfast2(P.gamma, res[RHO], res[M1], res[M2], res[EN], res[B1], res[B2], eb, rb,
+                                b1b, b2b, 1));
+      }
+  }
+  __shared__ double red[NTHREADS / 32][2];
+  for (int o = 16; o > 0; o >>= 1) {
+    cm0 = dmax0(cm0, __shfl_xor_sync(0xffffffffu, cm0, o));
+    cm1 = dmax0(cm1, __shfl_xor_sync(0xffffffffu, cm1, o));
+  }
+  if ((tid & 31) == 0) {
+    red[tid >> 5][0] = cm0;
+    red[tid >> 5][1] = cm1;
+  }
+  __syncthreads();
+  if (tid < 2) {
+    double v = 0.0;
+    for (int w = 0; w < NTHREADS / 32; w++) v = dmax0(v, red[w][tid]);
+    atomicMax(&B.cmax_out[tid], (unsigned long long)__double_as_longlong(v));
+  }
+}
+
+// launch helper: picks the background specialisation
+template <int MODE>
+static cudaError_t launch_stage2d(const KParams& K, const KBufs& B, cudaStream_t st) {
+  dim3 block(TX, TY);
+  dim3 grid((K.n0 - 4 + TX - 1) / TX, (K.n1 - 4 + TY - 1) / TY);
+  if (K.has_bg) {
+    stage2d_fast<MODE, true><<<grid, block, s2::smem_bytes<true>(), st>>>(K, B);
+  } else {
+    stage2d_fast<MODE, false><<<grid, block, s2::smem_bytes<false>(), st>>>(K, B);
+  }
+  return cudaGetLastError();
+}
+
+static cudaError_t stage2d_set_attributes() {
+  cudaError_t e;
+  if ((e = cudaFuncSetAttribute(stage2d_fast<SMAUG_INT_EULER, true>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s2::smem_bytes<true>())))
+    return e;
+  if ((e = cudaFuncSetAttribute(stage2d_fast<SMAUG_INT_EULER, false>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s2::smem_bytes<false>())))
+    return e;
+  if ((e = cudaFuncSetAttribute(stage2d_fast<SMAUG_INT_RK4, true>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s2::smem_bytes<true>())))
+    return e;
+  return cudaFuncSetAttribute(stage2d_fast<SMAUG_INT_RK4, false>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s2::smem_bytes<false>());
+}
