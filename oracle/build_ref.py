@@ -10,8 +10,9 @@ under /tmp, the build output goes to oracle/_ref/<name>/ (git-ignored).
 The reference's build selects a model by copying models/*.<model> over the
 compile-time parameter header and instantiates the shared device helpers by
 `sed s/MODID/<id>/` (src/Makefile:79-227); this recipe does the same for the
-Orszag-Tang model (`make ot`) with the run parameters substituted into
-include/iosmaugparams.h.  Three workarounds are needed with CUDA 12.9 / GCC 13:
+Orszag-Tang model (`make ot`, 2D) or the flux-tube model (`make fluxtube1`,
+3D with -DUSE_SAC_3D)
+with the run parameters substituted into include/iosmaugparams.h.  Three workarounds are needed with CUDA 12.9 / GCC 13:
   1. src/init.cu:169 passes an undeclared `w`; it is built with `wmod`
      (the only array in scope; the call is inside `if(p->readini==0)`,
      not taken when an .ini is read).
@@ -57,6 +58,10 @@ MODIDS = {
     "divb.cu": [("gradops.cu", "db"), ("dervfields.cu", "db")],
 }
 CFILES = ["iosmaug.c", "initialisation.c", "dxroutines.c", "readwrite.c"]
+# the flux-tube parameter header (Meta *metad) pairs with the C driver, whose
+# USE_SAC_3D branches allocate the z positions with nj entries (src/iosmaug.c:65-68),
+# so 3D builds need nk <= nj
+CFILES_3D = ["iosmaug.c", "initialisation.c", "dxroutines.c", "readwrite.c"]
 
 DEFAULTS = {
     "XMIN": "0.0", "XMAX": "6.283185307179586", "YMIN": "0.0", "YMAX": "6.283185307179586",
@@ -72,14 +77,17 @@ def _set_define(text, name, value):
     return pat.sub("#define %s %s" % (name, value), text)
 
 
-def build_ref(name, ni, nj, nt, arch="sm_100a", verbose=True, **kw):
+def build_ref(name, ni, nj, nt, arch="sm_100a", verbose=True, nk=None, **kw):
     if not os.path.isdir(REFROOT):
         raise RuntimeError("reference sources not present at %s" % REFROOT)
     cfg = dict(DEFAULTS)
     cfg.update({k.upper(): str(v) for k, v in kw.items()})
     dest = os.path.join(OUT, name)
     os.makedirs(dest, exist_ok=True)
-    stamp = "ni=%d nj=%d nt=%d %s arch=%s\n" % (ni, nj, nt, sorted(cfg.items()), arch)
+    three = nk is not None
+    if three and nk > nj:
+        raise ValueError("3D reference builds need nk <= nj")
+    stamp = "ni=%d nj=%d nk=%s nt=%d %s arch=%s\n" % (ni, nj, nk, nt, sorted(cfg.items()), arch)
     binp = os.path.join(dest, "smaug")
     stampf = os.path.join(dest, "build.txt")
     if os.path.exists(binp) and os.path.exists(stampf) and open(stampf).read() == stamp:
@@ -90,17 +98,26 @@ def build_ref(name, ni, nj, nt, arch="sm_100a", verbose=True, **kw):
             shutil.copytree(os.path.join(REFROOT, d), os.path.join(tmp, d))
         subprocess.check_call(["chmod", "-R", "u+w", tmp])
         src, inc, mod = (os.path.join(tmp, d) for d in ("src", "include", "models"))
-        # make ot (src/Makefile:98-101)
-        shutil.copy(os.path.join(mod, "iosmaugparams.h.ot"), os.path.join(inc, "iosmaugparams.h"))
-        shutil.copy(os.path.join(mod, "init_user.cu.ot"), os.path.join(src, "init_user.cu"))
-        shutil.copy(os.path.join(mod, "boundary.cu.ot"), os.path.join(src, "boundary.cu"))
+        model = "fluxtube1" if three else "ot"
+        # make ot / make fluxtube1 (src/Makefile:32-101)
+        shutil.copy(os.path.join(mod, "iosmaugparams.h." + model), os.path.join(inc, "iosmaugparams.h"))
+        shutil.copy(os.path.join(mod, "init_user.cu." + model), os.path.join(src, "init_user.cu"))
+        shutil.copy(os.path.join(mod, "boundary.cu." + model), os.path.join(src, "boundary.cu"))
+        if three:
+            shutil.copy(os.path.join(mod, "usersource.cu." + model), os.path.join(src, "usersource.cu"))
+            shutil.copy(os.path.join(mod, "initialisation_user.h.default"),
+                        os.path.join(inc, "initialisation_user.h"))
         ph = os.path.join(inc, "iosmaugparams.h")
         text = open(ph).read()
         text = _set_define(text, "NI", str(ni))
         text = _set_define(text, "NJ", str(nj))
         text = _set_define(text, "NT", str(nt))
-        for k in ("XMIN", "XMAX", "YMIN", "YMAX", "DT", "PCOURANT", "PMODDTON",
-                  "PCFGSAVEFREQUENCY", "PGAMMA", "CFGFILE", "CFGOUT"):
+        keys = ["XMIN", "XMAX", "YMIN", "YMAX", "DT", "PCOURANT", "PMODDTON",
+                "PCFGSAVEFREQUENCY", "PGAMMA", "CFGFILE", "CFGOUT"]
+        if three:
+            text = _set_define(text, "NK", str(nk))
+            keys += ["ZMIN", "ZMAX", "PGRAV0", "PGRAV1", "PGRAV2"]
+        for k in keys:
             text = _set_define(text, k, cfg[k])
         for k in ("PCHYP", "PCHYPRHO", "PCHYPENERGY", "PCHYPB0", "PCHYPB1", "PCHYPB2",
                   "PCHYPMOM0", "PCHYPMOM1", "PCHYPMOM2"):
@@ -120,18 +137,19 @@ def build_ref(name, ni, nj, nt, arch="sm_100a", verbose=True, **kw):
                 base = tpl[:-3]
                 open(os.path.join(inc, "%s_%s.cuh" % (base, mid)), "w").write(t)
         objs = []
+        sac = "-DUSE_SAC_3D" if three else "-DUSE_SAC"
         for cu in MODIDS:
             o = os.path.join(src, cu[:-3] + ".o")
-            cmd = ["nvcc", "-arch=" + arch, "-maxrregcount=32", "-DUSE_SAC", "-w",
+            cmd = ["nvcc", "-arch=" + arch, "-maxrregcount=32", sac, "-w",
                    "-Xcompiler", "-fno-unreachable-traps",
                    "-o", o, "-c", os.path.join(src, cu)]
             if verbose:
                 print(" ".join(cmd), flush=True)
             subprocess.check_call(cmd, cwd=src)
             objs.append(o)
-        for c in CFILES:
-            o = os.path.join(src, c[:-2] + ".o")
-            cmd = ["g++", "-O0", "-fno-unreachable-traps", "-DUSE_SAC", "-DD1D", "-w", "-fpermissive",
+        for c in (CFILES_3D if three else CFILES):
+            o = os.path.join(src, c.rsplit(".", 1)[0] + ".o")
+            cmd = ["g++", "-O0", "-fno-unreachable-traps", sac, "-DD1D", "-w", "-fpermissive",
                    "-o", o, "-c", os.path.join(src, c)]
             if verbose:
                 print(" ".join(cmd), flush=True)

@@ -137,7 +137,7 @@ static int init_O(O *o, const smaug_params_t *P) {
   o->n[1] = P->n[1];
   o->n[2] = (o->nd == 3) ? P->n[2] : 1;
   for (int d = 0; d < o->nd; d++)
-    if (o->n[d] < 9) return SMAUG_E_INVALID;
+    if (o->n[d] < 8) return SMAUG_E_INVALID;
   o->dimp = (long)o->n[0] * o->n[1] * o->n[2];
   setup_ids(o);
   for (int d = 0; d < 3; d++) {

@@ -23,6 +23,17 @@ change nu_r in the last interior column along dim 0.
 Each .npz holds the evolved fields (rho m1 m2 e b1 b2, ghosts included) of
 the initial state and of the saved steps, the positions, and the header
 times of the reference's .out files.
+
+3D cases (flux-tube model build, -DUSE_SAC_3D, contcd4 ghosts in every
+dimension, domain [0,0.1]^3, gravity -0.1 along dim 0, nonzero background
+fields, DT 1, courant 0.3, chyp 0.2, PGAMMA 1.66666667):
+  t3s      4x4x4 interior (8^3 = 512 cells: one thread block), 20 steps
+  t3a      12x12x8 interior (16x16x12 = 6 blocks), steps 0-5 and 10
+  t3b      20x12x8 interior (24x16x12 = 9 blocks), steps 0-3
+Every 3D grid holds a whole number of 512-thread blocks: the reference's
+contcd4 ghost kernels (models/boundary.cu.fluxtube1:16-85) have no
+cell-count guard, so a partial last block would write past the state array.
+The 3D fixtures hold all 13 fields (the backgrounds included).
 """
 import math
 import os
@@ -45,6 +56,64 @@ CASES = {
     "ot24x20": (24, 20, 5, 12, [0, 1, 2, 3, 4, 5]),
 }
 GAMMA_REF = 1.66666667  # models/iosmaugparams.h.ot PGAMMA
+
+# 3D: name: ((nx, ny, nz), seed, NT, steps kept, runs); runs > 1 repeats the
+# multi-block cases to expose order-dependent results
+L3 = 0.1
+G3 = -0.1
+CASES3 = {
+    "t3s": ((4, 4, 4), 21, 21, [1, 2, 3, 5, 10, 20], 1),
+    "t3a": ((12, 12, 8), 22, 12, [0, 1, 2, 3, 4, 5, 10], 2),
+    "t3b": ((20, 12, 8), 23, 5, [0, 1, 2, 3], 2),
+}
+
+
+def tube_state(nx, ny, nz, seed, gamma=GAMMA_REF):
+    """Smooth 3D state with nonzero backgrounds on [0, L3]^3: stratified-like
+    rho_b, p_b along dim 0, a uniform-plus-sinusoid background field, and
+    O(1e-2..1e-1) perturbations; positive pressure everywhere."""
+    import smaug_b200.ic as I
+    x, _ = I._axis(nx, 0, L3)
+    y, _ = I._axis(ny, 0, L3)
+    z, _ = I._axis(nz, 0, L3)
+    Z, Y, X = np.meshgrid(z, y, x, indexing="ij")
+    k = 2 * math.pi / L3
+    rng = np.random.default_rng(seed)
+    w = np.zeros((13,) + X.shape)
+    rhob = 1.0 + 0.2 * np.cos(k * X)
+    pb = 1.0 + 0.1 * np.cos(k * X)
+    bb = [0.3 + 0 * X, 0.05 * np.cos(k * Y), 0.02 * np.sin(k * Z)]
+    rho = 0.01 * np.sin(k * X) * np.sin(k * Y) * np.cos(k * Z)
+    rho = rho + 1e-3 * rhob * rng.standard_normal(X.shape)
+    v = [0.1 * np.sin(k * Y), 0.1 * np.sin(k * Z), 0.1 * np.sin(k * X)]
+    b = [0.05 * np.cos(k * Z), 0.05 * np.cos(k * X), 0.05 * np.cos(k * Y)]
+    pp = 0.02 * (1.0 + 0.5 * np.sin(k * X + k * Y))
+    rt = rho + rhob
+    eb = pb / (gamma - 1) + 0.5 * sum(c * c for c in bb)
+    et = (pb + pp) / (gamma - 1) + 0.5 * rt * sum(c * c for c in v) + \
+        0.5 * sum((bb[d] + b[d]) ** 2 for d in range(3))
+    w[0] = rho
+    for d in range(3):
+        w[1 + d] = rt * v[d]
+        w[5 + d] = b[d]
+        w[10 + d] = bb[d]
+    w[4] = et - eb
+    w[8] = eb
+    w[9] = rhob
+    return w, np.stack([X, Y, Z])
+
+
+def _build3(name, nx, ny, nz, nt):
+    from oracle import build_ref
+    return build_ref.build_ref(name, nx, ny, nt, nk=nz, verbose=False,
+                               XMIN="0.0", XMAX=repr(L3), YMIN="0.0", YMAX=repr(L3),
+                               ZMIN="0.0", ZMAX=repr(L3), PGRAV0=repr(G3), PGRAV1="0.0",
+                               PGRAV2="0.0")
+
+
+def _selected(table):
+    want = sys.argv[2].split(",") if len(sys.argv) > 2 else None
+    return {k: v for k, v in table.items() if want is None or k in want}
 
 
 def ot_state(nx, ny, seed, noise=1e-3):
@@ -69,30 +138,57 @@ def prepare():
     from smaug_b200 import formats
     from oracle import build_ref
     os.makedirs(WORK, exist_ok=True)
-    for name, (nx, ny, seed, nt, keep) in CASES.items():
+    for name, (nx, ny, seed, nt, keep) in _selected(CASES).items():
         w, pos = ot_state(nx, ny, seed)
         formats.write_ini(os.path.join(WORK, name + ".ini"), w, pos)
         build_ref.build_ref(name, nx, ny, nt, verbose=False)
         print("prepared", name)
+    for name, ((nx, ny, nz), seed, nt, keep, runs) in _selected(CASES3).items():
+        w, pos = tube_state(nx, ny, nz, seed)
+        formats.write_ini(os.path.join(WORK, name + ".ini"), w, pos, gamma=GAMMA_REF,
+                          g=(G3, 0.0, 0.0))
+        _build3(name, nx, ny, nz, nt)
+        print("prepared", name)
+
+
+def _run_one(name, keep, tag=""):
+    from oracle import run_ref
+    binp = os.path.join(ROOT, "oracle", "_ref", name, "smaug")
+    rundir = os.path.join("/tmp", "gold_" + name + tag)
+    rc, times = run_ref.run(binp, os.path.join(WORK, name + ".ini"), rundir,
+                            keep=set(keep) | {0})
+    dest = os.path.join(RUNS, name + tag)
+    os.makedirs(dest, exist_ok=True)
+    os.system("cp -r %s/out %s/times.txt %s/stdout_tail.txt %s/" % (rundir, rundir, rundir, dest))
+    print(name + tag, "rc", rc, "steps", len(times))
+    if rc:
+        sys.exit(rc)
 
 
 def run():
-    from oracle import run_ref
-    for name, (nx, ny, seed, nt, keep) in CASES.items():
-        binp = os.path.join(ROOT, "oracle", "_ref", name, "smaug")
-        rundir = os.path.join("/tmp", "gold_" + name)
-        rc, times = run_ref.run(binp, os.path.join(WORK, name + ".ini"), rundir, keep=set(keep) | {0})
-        dest = os.path.join(RUNS, name)
-        os.makedirs(dest, exist_ok=True)
-        os.system("cp -r %s/out %s/times.txt %s/" % (rundir, rundir, dest))
-        print(name, "rc", rc, "steps", len(times))
-        if rc:
-            sys.exit(rc)
+    for name, (nx, ny, seed, nt, keep) in _selected(CASES).items():
+        _run_one(name, keep)
+    for name, (n, seed, nt, keep, runs) in _selected(CASES3).items():
+        for r in range(runs):
+            _run_one(name, keep, "" if r == 0 else "_r%d" % r)
 
 
 def collect():
     from smaug_b200 import formats
-    for name, (nx, ny, seed, nt, keep) in CASES.items():
+    for name, ((nx, ny, nz), seed, nt, keep, runs) in _selected(CASES3).items():
+        w0, pos0, _ = formats.read_ini(os.path.join(WORK, name + ".ini"), 3)
+        states, times = [], []
+        for k in keep:
+            w, pos, h = formats.read_out(os.path.join(RUNS, name, "out", "ref_%d.out" % k))
+            states.append(w)
+            times.append(h["t"])
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), w0=w0, pos=pos0,
+                            steps=np.array(keep), states=np.array(states),
+                            hdr_t=np.array(times), gamma=GAMMA_REF,
+                            dx=np.array([L3 / nx, L3 / ny, L3 / nz]),
+                            g=np.array([G3, 0.0, 0.0]))
+        print("wrote", name)
+    for name, (nx, ny, seed, nt, keep) in _selected(CASES).items():
         w0, pos0, _ = formats.read_ini(os.path.join(WORK, name + ".ini"), 2)
         states, times = [], []
         for k in keep:

@@ -8,11 +8,15 @@ from smaug_b200 import params as P
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 STRICT = ("g16", "g18x12", "ot64")     # full multi-step runs
 ONESTEP = ("ot24x20",)                 # consecutive steps, one-step parity
+STRICT3 = ("t3s", "t3a", "t3b")        # 3D flux-tube build, contcd4 ghosts, backgrounds
 
 
 def load(name):
     z = np.load(os.path.join(GOLDEN, name + ".npz"))
     d = {k: z[k] for k in z.files}
+    if d["w0"].ndim == 4:          # 3D fixtures hold all 13 fields
+        d["w0full"] = d["w0"].copy()
+        return d
     w0 = np.zeros((10,) + d["w0"].shape[1:])
     w0[:6] = d["w0"]
     d["w0full"] = w0
@@ -20,8 +24,13 @@ def load(name):
 
 
 def params(d, **kw):
-    ny, nx = d["w0"].shape[1:]
     kw.setdefault("integrator", P.INT_EULER)
+    if d["w0"].ndim == 4:
+        nz, ny, nx = d["w0"].shape[1:]
+        return P.make_params(ndim=3, n=(nx, ny, nz), dx=tuple(d["dx"]),
+                             gamma=float(d["gamma"]), courant=0.3, dtmax=1.0, dt=1e-8,
+                             g=tuple(d["g"]), boundtype=[[P.BC_CONTCD4] * 2] * 3, **kw)
+    ny, nx = d["w0"].shape[1:]
     return P.make_params(ndim=2, n=(nx, ny, 1), dx=tuple(d["dx"]), gamma=float(d["gamma"]),
                          courant=0.3, dtmax=1.0, dt=1e-8, **kw)
 

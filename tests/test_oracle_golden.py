@@ -47,6 +47,24 @@ def test_oracle_one_step_multiblock(oracle, name):
             assert err <= TOL, (name, steps[b], f, err)
 
 
+@pytest.mark.parametrize("name", G.STRICT3)
+def test_oracle_matches_reference_run_3d(oracle, name):
+    """3D: every one of the 13 fields (backgrounds included) at every saved
+    step of the reference's flux-tube build (-DUSE_SAC_3D, contcd4 ghosts in
+    all dimensions, gravity along dim 0)."""
+    d = G.load(name)
+    p = G.params(d)
+    run = oracle.OracleRun(p, d["w0full"], d["pos"])
+    done = 0
+    for k, ref in zip(d["steps"], d["states"]):
+        run.advance(int(k) - done)
+        done = int(k)
+        for f in range(13):
+            assert rel_l2(run.w[f], ref[f]) <= TOL, (name, k, f, rel_l2(run.w[f], ref[f]))
+    nxt = oracle.OracleRun(p, d["w0full"], d["pos"]).advance(int(d["steps"][-1]) + 1)
+    assert abs(nxt.t - d["hdr_t"][-1]) <= 1e-14 * abs(d["hdr_t"][-1])
+
+
 def test_zero_pad_model_does_not_match(oracle):
     """The pad race matters: the zero-pad model misses the reference."""
     from smaug_b200 import params as P
