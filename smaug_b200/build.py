@@ -7,8 +7,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libsmaug_b200.so")
 SRCS = [os.path.join(HERE, "csrc", f) for f in ("engine.cu", "host_io.cpp")]
-DEPS = SRCS + [os.path.join(HERE, "csrc", "engine_internal.h"),
-               os.path.join(ROOT, "include", "smaug_b200.h")]
+DEPS = SRCS + [os.path.join(HERE, "csrc", f) for f in sorted(os.listdir(os.path.join(HERE, "csrc")))
+               if f.endswith((".h", ".cuh"))] + [os.path.join(ROOT, "include", "smaug_b200.h")]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -1,7 +1,8 @@
 // engine.cu -- B200 (sm_100a) time-advance engine for SMAUG, FP64.
 //
 // One fused kernel per stage evaluates the whole spatial operator of the
-// reference's single-stage step (src/iosmaug.c:631-835) for a 2D tile:
+// reference's single-stage step (src/iosmaug.c:631-835) for a 2D tile
+// (stage2d.cuh) or a 3D tile (stage3d.cuh):
 //   state tile + 3-cell halo staged in shared memory
 //   -> directional fluxes + 4th-order divergence     (src/centdiff1.cu, centdiff2.cu)
 //   -> background energy coupling, gravity            (src/centdiff2.cu:80-154)
@@ -31,7 +32,7 @@
 #include "../../include/smaug_b200.h"
 #include "engine_internal.h"
 
-#define SMAUG_VERSION_STRING "smaug_b200 0.1 (sm_100a, fp64)"
+#define SMAUG_VERSION_STRING "smaug_b200 0.2 (sm_100a, fp64, 2D+3D)"
 
 namespace smaug {
 
@@ -76,7 +77,7 @@ constexpr int NF2 = 10;            // 2D fields: 6 evolved + 4 background
 enum { RHO = 0, M1 = 1, M2 = 2, EN = 3, B1 = 4, B2 = 5, EB = 6, RHOB = 7, BB1 = 8, BB2 = 9 };
 
 struct KParams {
-  int n0, n1;
+  int n0, n1, n2;   // n2 = 1 in 2D
   long ncell;
   int bt[3];        // boundtype[dim][0] (upper) -- gradient edge zeroing
   int bc[3];        // ghost-fill type per dim
@@ -195,6 +196,11 @@ __device__ __forceinline__ bool zero1n(int a, int n) {
 #include "stage2d.cuh"
 
 // ---------------------------------------------------------------------------
+// 3D stage kernel
+// ---------------------------------------------------------------------------
+#include "stage3d.cuh"
+
+// ---------------------------------------------------------------------------
 // auxiliary kernels: ghost fill and CFL maxima of an arbitrary state
 // ---------------------------------------------------------------------------
 // source interior index of a ghost index (inverse of ghost_images)
@@ -218,6 +224,37 @@ __global__ void ghost_fill2d_kernel(const KParams P, double* u) {
   if (si == i && sj == j) return;
   long s = (long)sj * P.n0 + si;
   for (int f = 0; f < 6; f++) u[f * P.ncell + c] = u[f * P.ncell + s];
+}
+
+__global__ void ghost_fill3d_kernel(const KParams P, double* u) {
+  long c = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (c >= P.ncell) return;
+  int i = (int)(c % P.n0), j = (int)((c / P.n0) % P.n1), k = (int)(c / ((long)P.n0 * P.n1));
+  int si = ghost_source(i, P.n0, P.bc[0]);
+  int sj = ghost_source(j, P.n1, P.bc[1]);
+  int sk = ghost_source(k, P.n2, P.bc[2]);
+  if (si == i && sj == j && sk == k) return;
+  long s = ((long)sk * P.n1 + sj) * P.n0 + si;
+  for (int f = 0; f < 8; f++) u[f * P.ncell + c] = u[f * P.ncell + s];
+}
+
+__global__ void cmax3d_kernel(const KParams P, const double* u, const double* bg,
+                              unsigned long long* out) {
+  long c = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  double cm[3] = {0, 0, 0};
+  if (c < P.ncell) {
+    const long nc = P.ncell;
+    double s[8], g[5];
+    for (int f = 0; f < 8; f++) s[f] = u[f * nc + c];
+    for (int f = 0; f < 5; f++) g[f] = bg[f * nc + c];
+    for (int d = 0; d < 3; d++) cm[d] = cfast3(P.gamma, s, g, d);
+  }
+  for (int d = 0; d < 3; d++) {
+    double v = cm[d];
+    if (!(v > 0)) v = 0.0;
+    for (int o = 16; o > 0; o >>= 1) v = dmax0(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(&out[d], (unsigned long long)__double_as_longlong(v));
+  }
 }
 
 __global__ void cmax2d_kernel(const KParams P, const double* u, const double* bg,
@@ -290,10 +327,9 @@ static int validate(const smaug_params_t* p) {
   if (p->version != SMAUG_PARAMS_VERSION)
     return set_error(SMAUG_E_INVALID, "parameter block version %d, expected %d", p->version,
                      SMAUG_PARAMS_VERSION);
-  if (p->ndim == 3) return set_error(SMAUG_E_UNSUPPORTED, "3D is not implemented in this build");
-  if (p->ndim != 2) return set_error(SMAUG_E_INVALID, "ndim must be 2 or 3 (got %d)", p->ndim);
+  if (p->ndim != 2 && p->ndim != 3) return set_error(SMAUG_E_INVALID, "ndim must be 2 or 3 (got %d)", p->ndim);
   for (int d = 0; d < p->ndim; d++)
-    if (p->n[d] < 9) return set_error(SMAUG_E_INVALID, "n[%d]=%d: need at least 5 interior cells", d, p->n[d]);
+    if (p->n[d] < 8) return set_error(SMAUG_E_INVALID, "n[%d]=%d: need at least 4 interior cells", d, p->n[d]);
   if (p->integrator != SMAUG_INT_EULER && p->integrator != SMAUG_INT_RK4)
     return set_error(SMAUG_E_INVALID, "unknown integrator %d", p->integrator);
   if (p->precision != SMAUG_PREC_FP64)
@@ -337,6 +373,20 @@ static std::vector<int> pad_sources(const smaug_params_t* p, int dim) {
       long t = L - off;
       if (p->pad_model == SMAUG_PAD_STRAY && t >= 0 && t < dimp) src[r] = (int)t;
     }
+  } else {
+    // across index: the two other coordinates, lower axis fastest
+    int a1 = dim == 0 ? 1 : 0, a2 = dim == 2 ? 1 : 2;
+    src.assign(n[a1] * n[a2], -1);
+    for (long v = 0; v < n[a2]; v++)
+      for (long u = 0; u < n[a1]; u++) {
+        long P[3];
+        P[dim] = n[dim] + 1;
+        P[a1] = u + 1;
+        P[a2] = v + 1;
+        long L = (P[2] * m[1] + P[1]) * m[0] + P[0];
+        long t = L - off;
+        if (p->pad_model == SMAUG_PAD_STRAY && t >= 0 && t < dimp) src[v * n[a1] + u] = (int)t;
+      }
   }
   return src;
 }
@@ -359,39 +409,42 @@ static int create(const smaug_params_t* p, const double* w, const double* pos, E
   std::vector<double> delx((size_t)e->nd * nc);
   grid_metric(e->nd, p->n, e->pos_host.data(), delx.data());
   std::vector<double> dl1[3], ps1[3];
+  const int n2 = (e->nd == 3) ? p->n[2] : 1;
   for (int d = 0; d < e->nd; d++) {
     dl1[d].assign(p->n[d], 0.0);
     ps1[d].assign(p->n[d], 0.0);
     // representative interior line; every interior cell must agree
-    int rep[2] = {2, 2};
     for (int a = 0; a < p->n[d]; a++) {
-      int ij[2] = {rep[0], rep[1]};
-      ij[d] = a;
-      long c = (long)ij[1] * p->n[0] + ij[0];
+      int ijk[3] = {2, 2, e->nd == 3 ? 2 : 0};
+      ijk[d] = a;
+      long c = ((long)ijk[2] * p->n[1] + ijk[1]) * p->n[0] + ijk[0];
       dl1[d][a] = delx[(size_t)d * nc + c];
       ps1[d][a] = e->pos_host[(size_t)d * nc + c];
     }
-    for (int j = 2; j <= p->n[1] - 3; j++)
-      for (int i = 2; i <= p->n[0] - 3; i++) {
-        long c = (long)j * p->n[0] + i;
-        int a = (d == 0) ? i : j;
-        if (delx[(size_t)d * nc + c] != dl1[d][a] ||
-            (p->driver != SMAUG_DRIVER_NONE && e->pos_host[(size_t)d * nc + c] != ps1[d][a])) {
-          delete e;
-          return set_error(SMAUG_E_UNSUPPORTED,
-                           "grid metric along dim %d varies across lines (cell %d,%d); only "
-                           "tensor-product grids are supported", d, i, j);
+    const int klo = (e->nd == 3) ? 2 : 0, khi = (e->nd == 3) ? n2 - 3 : 0;
+    for (int k = klo; k <= khi; k++)
+      for (int j = 2; j <= p->n[1] - 3; j++)
+        for (int i = 2; i <= p->n[0] - 3; i++) {
+          long c = ((long)k * p->n[1] + j) * p->n[0] + i;
+          int a = (d == 0) ? i : (d == 1 ? j : k);
+          if (delx[(size_t)d * nc + c] != dl1[d][a] ||
+              (p->driver != SMAUG_DRIVER_NONE && e->pos_host[(size_t)d * nc + c] != ps1[d][a])) {
+            delete e;
+            return set_error(SMAUG_E_UNSUPPORTED,
+                             "grid metric along dim %d varies across lines (cell %d,%d,%d); only "
+                             "tensor-product grids are supported", d, i, j, k);
+          }
+          if (!(dl1[d][a] > 0)) {
+            delete e;
+            return set_error(SMAUG_E_INVALID, "non-positive cell width along dim %d at %d", d, a);
+          }
         }
-        if (!(dl1[d][a] > 0)) {
-          delete e;
-          return set_error(SMAUG_E_INVALID, "non-positive cell width along dim %d at %d", d, a);
-        }
-      }
   }
   // kernel parameters
   KParams& K = e->K;
   K.n0 = p->n[0];
   K.n1 = p->n[1];
+  K.n2 = n2;
   K.ncell = nc;
   for (int d = 0; d < 3; d++) {
     K.bt[d] = (d < e->nd) ? p->boundtype[d][0] : 0;
@@ -455,6 +508,7 @@ static int create(const smaug_params_t* p, const double* w, const double* pos, E
   E_TRY(cudaMemcpy(e->d_t, t0, sizeof(t0), cudaMemcpyHostToDevice));
   E_TRY(cudaMemset(e->d_flags, 0, sizeof(int)));
   E_TRY(stage2d_set_attributes());
+  E_TRY(stage3d_set_attributes());
 #undef E_TRY
   *out = e;
   return SMAUG_OK;
@@ -464,11 +518,17 @@ static int create(const smaug_params_t* p, const double* w, const double* pos, E
 static int reset_derived(Engine* e) {
   const int bs = 256;
   long nb = (e->ncell + bs - 1) / bs;
-  ghost_fill2d_kernel<<<(unsigned)nb, bs, 0, e->stream>>>(e->K, e->d_u[e->cur]);
+  if (e->nd == 3)
+    ghost_fill3d_kernel<<<(unsigned)nb, bs, 0, e->stream>>>(e->K, e->d_u[e->cur]);
+  else
+    ghost_fill2d_kernel<<<(unsigned)nb, bs, 0, e->stream>>>(e->K, e->d_u[e->cur]);
   CUDA_TRY(cudaGetLastError());
   CUDA_TRY(cudaMemsetAsync(e->d_cmax, 0, sizeof(unsigned long long) * 9, e->stream));
   unsigned long long* slot = e->d_cmax + 3 * (e->stage_count % 3);
-  cmax2d_kernel<<<(unsigned)nb, bs, 0, e->stream>>>(e->K, e->d_u[e->cur], e->d_bg, slot);
+  if (e->nd == 3)
+    cmax3d_kernel<<<(unsigned)nb, bs, 0, e->stream>>>(e->K, e->d_u[e->cur], e->d_bg, slot);
+  else
+    cmax2d_kernel<<<(unsigned)nb, bs, 0, e->stream>>>(e->K, e->d_u[e->cur], e->d_bg, slot);
   CUDA_TRY(cudaGetLastError());
   return SMAUG_OK;
 }
@@ -496,10 +556,17 @@ static int launch_stage(Engine* e, int mode, int stage, const double* uin, const
   B.flags = e->d_flags;
   B.mode = mode;
   B.stage = stage;
-  if (mode == SMAUG_INT_EULER)
-    CUDA_TRY(launch_stage2d<SMAUG_INT_EULER>(e->K, B, e->stream));
-  else
-    CUDA_TRY(launch_stage2d<SMAUG_INT_RK4>(e->K, B, e->stream));
+  if (e->nd == 3) {
+    if (mode == SMAUG_INT_EULER)
+      CUDA_TRY(launch_stage3d<SMAUG_INT_EULER>(e->K, B, e->stream));
+    else
+      CUDA_TRY(launch_stage3d<SMAUG_INT_RK4>(e->K, B, e->stream));
+  } else {
+    if (mode == SMAUG_INT_EULER)
+      CUDA_TRY(launch_stage2d<SMAUG_INT_EULER>(e->K, B, e->stream));
+    else
+      CUDA_TRY(launch_stage2d<SMAUG_INT_RK4>(e->K, B, e->stream));
+  }
   e->stage_count++;
   return SMAUG_OK;
 }
@@ -768,6 +835,7 @@ extern "C" int smaug_euler_step_noalloc(const smaug_params_t* p, const double* w
   int rc = validate(p);
   if (rc) return rc;
   if (!w_in || !w_out || !delx || !dt) return set_error(SMAUG_E_INVALID, "null argument");
+  if (p->ndim != 2) return set_error(SMAUG_E_UNSUPPORTED, "the allocation-free step is 2D only");
   if (w_in == w_out) return set_error(SMAUG_E_INVALID, "w_in and w_out must not alias");
   if (p->n[0] > NOALLOC_MAXN || p->n[1] > NOALLOC_MAXN)
     return set_error(SMAUG_E_UNSUPPORTED,
@@ -783,6 +851,7 @@ extern "C" int smaug_euler_step_noalloc(const smaug_params_t* p, const double* w
   KParams K{};
   K.n0 = p->n[0];
   K.n1 = p->n[1];
+  K.n2 = 1;
   K.ncell = nc;
   for (int d = 0; d < 3; d++) {
     K.bt[d] = (d < 2) ? p->boundtype[d][0] : 0;

@@ -25,9 +25,9 @@ def test_invalid_params_rejected(engine_lib):
         engine_lib.Engine(p, w, pos)
     assert e.value.code == 1
     p = params_for(w, dx)
-    p.n[0] = 8
+    p.n[0] = 7
     with pytest.raises((engine_lib.SmaugError, ValueError)):
-        engine_lib.Engine(p, w[:, :, :8].copy(), pos[:, :, :8].copy())
+        engine_lib.Engine(p, w[:, :, :7].copy(), pos[:, :, :7].copy())
 
 
 def test_null_handle(engine_lib):
@@ -89,10 +89,36 @@ def test_write_out(engine_lib, tmp_path):
     e.close()
 
 
-def test_3d_reports_unsupported(engine_lib):
-    p = P.make_params(ndim=3, n=(12, 12, 12))
-    w = np.zeros((13, 12, 12, 12))
-    pos = np.zeros((3, 12, 12, 12))
+def test_3d_roundtrip_and_write_out(engine_lib, tmp_path):
+    from tests.util import params3, state3d
+    w, pos, dx = state3d(9, 7, 6, seed=4)
+    p = params3(w, dx)
+    e = engine_lib.Engine(p, w, pos)
+    e.step(2)
+    st = e.state()
+    assert st.shape == (13, 10, 11, 13)
+    assert np.array_equal(st[8:], w[8:])          # backgrounds carried unchanged
+    e.set_state(st)
+    assert np.array_equal(e.state(), st)
+    path = str(tmp_path / "s3.out")
+    e.write_out(path, name="tube", it=2, t=0.25)
+    w2, pos2, hdr = formats.read_out(path)
+    assert np.array_equal(w2, st)
+    assert hdr["ndim"] == 3 and hdr["nw"] == 13 and hdr["n"] == [13, 11, 10]
+    e.close()
+
+
+def test_3d_too_small_is_rejected(engine_lib):
+    p = P.make_params(ndim=3, n=(12, 12, 7))
     with pytest.raises(engine_lib.SmaugError) as e:
-        engine_lib.Engine(p, w, pos)
+        engine_lib.Engine(p, np.zeros((13, 7, 12, 12)), np.zeros((3, 7, 12, 12)))
+    assert e.value.code == 1
+
+
+def test_noalloc_rejects_3d(engine_lib):
+    """Rejected on the parameter block, before any pointer is used."""
+    p = P.make_params(ndim=3, n=(12, 12, 12))
+    d = np.zeros(36)
+    with pytest.raises(engine_lib.SmaugError) as e:
+        engine_lib.euler_step_noalloc(p, 1, 2, d, 1e-3)
     assert e.value.code == 6

@@ -54,3 +54,25 @@ def params_for(w, dx, **kw):
     kw.setdefault("courant", 0.3)
     kw.setdefault("dtmax", 1.0)
     return P.make_params(ndim=2, n=(n[0], n[1], 1), dx=dx, **kw)
+
+
+def state3d(nx, ny, nz, seed=0, background=True):
+    """3D state on [0,0.1]^3 (the generator of the 3D golden fixtures):
+    nonzero backgrounds, or with background=False the same total state folded
+    into the perturbation fields.  Returns (w[13], pos[3], dx)."""
+    from tests.golden.make_golden import L3, tube_state
+    w, pos = tube_state(nx, ny, nz, seed)
+    if not background:
+        w[0] += w[9]
+        w[4] += w[8]
+        for c in range(3):
+            w[5 + c] += w[10 + c]
+        w[8:] = 0.0
+    return w, pos, (L3 / nx, L3 / ny, L3 / nz)
+
+
+def params3(w, dx, boundtype=(P.BC_CONTCD4,) * 3, **kw):
+    n = list(reversed(w.shape[1:]))
+    kw.setdefault("courant", 0.3)
+    kw.setdefault("dtmax", 1.0)
+    return P.make_params(ndim=3, n=tuple(n), dx=dx, boundtype=boundtype, **kw)
