@@ -13,6 +13,12 @@ buffer) is far larger than the 126 MB L2, so no flush is needed between steps.
 N>1 (torchrun): replicas only -- each rank advances its own copy, no
 collective on the data path; value = total cell updates / max rank time.
 
+--workload tube: the 3D stratified solar atmosphere instead (256^3 interior
+cells by default, --n sets it): vertical axis = dim 0 (contcd4 ghosts),
+periodic x and y, hydrostatic background on 2 x 2 x 6 Mm with a uniform
+10 G vertical field, Gaussian vertical-velocity driver (200 m/s, 30 s period,
+sigma 0.2 Mm, centred at z = 0.1 Mm, x = y = 1 Mm), gravity 274 m/s^2.
+
 --impl reference: the reference has no CPU solver (every routine is a CUDA
 kernel), so the CPU baseline is the oracle, the FP64 restatement of the
 reference's kernels (oracle/), run with all host threads on a bounded
@@ -32,13 +38,18 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 WORKLOAD_N = 4096
+TUBE_N = 256
 METRIC = "Mcell-updates/s per RK4 step"
 UNIT = "Mcell-updates/s"
-# algorithmic HBM bytes per interior cell per RK4 step (FP64, 2D: P=6
-# evolved, B=4 background fields): stage 0 reads Un,B writes U2,Acc (3P+B);
-# stages 1-2 read Us,Un,Acc,B write Us+1,Acc (5P+B); stage 3 reads U4,Acc,B
-# writes Un+1 (3P+B) -> 16P+4B = 112 doubles
-ALG_BYTES_PER_CELL_STEP = (16 * 6 + 4 * 4) * 8
+
+
+def alg_bytes_per_cell_step(ndim):
+    """Algorithmic HBM bytes per interior cell per RK4 step, FP64: P evolved
+    and B background fields; stage 0 reads Un,B writes U2,Acc (3P+B); stages
+    1-2 read Us,Un,Acc,B write Us+1,Acc (5P+B); stage 3 reads U4,Acc,B writes
+    Un+1 (3P+B) -> 16P+4B doubles (2D: 112, 3D: 148)."""
+    P, B = 2 + 2 * ndim, 2 + ndim
+    return (16 * P + 4 * B) * 8
 
 
 def peaks():
@@ -102,6 +113,31 @@ def make_case(N, seed=1):
     p = P.make_params(ndim=2, n=(N + 4, N + 4, 1), dx=dx, courant=0.3, dtmax=1.0,
                       integrator=P.INT_RK4)
     return p, w, pos
+
+
+def make_tube(N, seed=1):
+    """3D stratified atmosphere, N^3 interior cells, 2 x 2 x 6 Mm (dim 0 vertical)."""
+    from smaug_b200 import ic, params as P
+    w, pos, dx = ic.stratified(nz=N, nx=N, ny=N, seed=seed)
+    p = P.make_params(ndim=3, n=(N + 4, N + 4, N + 4), dx=dx, courant=0.3, dtmax=1.0,
+                      integrator=P.INT_RK4, g=(-274.0, 0.0, 0.0),
+                      boundtype=(P.BC_CONTCD4, P.BC_PERIODIC, P.BC_PERIODIC),
+                      driver=P.DRIVER_GAUSS, drv_amp=200.0, drv_period=30.0,
+                      drv_x0=(0.1e6, 1.0e6, 1.0e6), drv_sigma=(0.2e6, 0.2e6, 0.2e6))
+    return p, w, pos
+
+
+def workload(args, seed=1):
+    """(params, w, pos, interior cells, description) of the selected workload."""
+    N = args.n
+    if args.workload == "tube":
+        p, w, pos = make_tube(N, seed)
+        return p, w, pos, N ** 3, ("3D stratified atmosphere %dx%dx%d (+2 ghost layers), 2x2x6 Mm, "
+                                   "contcd4 vertical / periodic horizontal, gravity, Gaussian "
+                                   "driver, hyperdiffusion, CFL 0.3, FP64, classical RK4" % (N, N, N))
+    p, w, pos = make_case(N, seed)
+    return p, w, pos, N * N, ("2D Orszag-Tang %dx%d (+2 ghost layers), periodic, "
+                              "hyperdiffusion, CFL 0.3, FP64, classical RK4" % (N, N))
 
 
 def dist_setup(args):
@@ -196,13 +232,16 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--n", type=int, default=WORKLOAD_N)
+    ap.add_argument("--workload", default="ot", choices=["ot", "tube"])
+    ap.add_argument("--n", type=int, default=None)
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--ref-sample", type=int, default=512)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ref-gpu", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.n is None:
+        args.n = TUBE_N if args.workload == "tube" else WORKLOAD_N
     ws, rank, local = dist_setup(args)
     if args.impl == "reference":
         reference_arm(args, ws, rank)
@@ -217,13 +256,13 @@ def main():
 
     torch.cuda.set_device(local)
     N = args.n
-    p, w, pos = make_case(N, seed=1 + rank)
+    p, w, pos, ncell_int, desc = workload(args, seed=1 + rank)
     eng = engine.Engine(p, w, pos)
     # a dedicated stream: the engine launches on it, the events are recorded on it
     stream = torch.cuda.Stream()
     assert stream.cuda_stream != 0
     eng.set_stream(stream.cuda_stream)
-    ncell_int = N * N
+    alg_bytes = alg_bytes_per_cell_step(p.ndim)
 
     def barrier():
         if ws > 1:
@@ -277,23 +316,23 @@ def main():
         dist.all_reduce(te, op=dist.ReduceOp.MAX)
     e2e_ms = float(te.item())
     e2e_val = ncell_int * args.e2e_steps * ws / (e2e_ms / 1e3) / 1e6
-    h2d = 6 * p.ncells * 8
+    h2d = (2 + 2 * p.ndim) * p.ncells * 8
     d2h = nvar * p.ncells * 8
     eng.close()
 
     if rank == 0:
         peak, pk_kind = peaks()
-        achieved = ALG_BYTES_PER_CELL_STEP * ncell_int * args.steps / (ms / 1e3) / 1e9
+        achieved = alg_bytes * ncell_int * args.steps / (ms / 1e3) / 1e9
+        state_gb = (2 + 2 * p.ndim) * p.ncells * 8 / 1e9
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "2D Orszag-Tang %dx%d (+2 ghost layers), periodic, "
-                                   "hyperdiffusion, CFL 0.3, FP64, classical RK4" % (N, N),
+            "config": {"workload": desc,
                        "interior_cells": ncell_int, "integrator": "rk4", "precision": "fp64",
                        "parallelism": "replicas" if ws > 1 else "single-gpu",
-                       "l2": "state 0.8 GB per buffer > 126 MB L2, no flush"},
+                       "l2": "state %.2f GB per buffer > 126 MB L2, no flush" % state_gb},
             "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "steps": args.e2e_steps,
                     "path": "smaug_set_state + smaug_step + smaug_get_state, pinned host buffers",
@@ -302,18 +341,18 @@ def main():
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": None,
                          "peak_kind": pk_kind,
-                         "alg_bytes_per_cell_step": ALG_BYTES_PER_CELL_STEP,
+                         "alg_bytes_per_cell_step": alg_bytes,
                          "note": "stage kernel; FP64 arithmetic, not HBM, limits this form"},
             "clocks": clk.summary(),
         }
-        if ws == 1 and not args.no_cpu_baseline:
+        if ws == 1 and not args.no_cpu_baseline and args.workload == "ot":
             os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
             v, el, thr = cpu_sample(args.ref_sample, 1)
             line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": thr, "kind": "port",
                                     "sample": "1 RK4 step of a %dx%d Orszag-Tang grid (%.1f s), "
                                               "oracle/smaug_oracle.c, OpenMP" % (
                                                   args.ref_sample, args.ref_sample, el)}
-        if ws == 1 and not args.no_ref_gpu:
+        if ws == 1 and not args.no_ref_gpu and args.workload == "ot":
             line["reference_gpu"] = reference_gpu_binary()
         print(json.dumps(line), flush=True)
     if ws > 1:
