@@ -10,6 +10,10 @@ buffer) is far larger than the 126 MB L2, so no flush is needed between steps.
          the engine's stream (torch's current stream is handed to the engine)
   e2e    the same metric through the C ABI with host buffers: per step
          smaug_set_state (pinned H2D) + smaug_step + smaug_get_state (D2H)
+  mixed  the mixed precision form (float perturbation storage and
+         hyperdiffusion, double elsewhere) on the same workload, timed the
+         same way, with its relative L2 distance per field from the FP64
+         state after the same number of steps
 N>1 (torchrun): replicas only -- each rank advances its own copy, no
 collective on the data path; value = total cell updates / max rank time.
 
@@ -41,6 +45,16 @@ WORKLOAD_N = 4096
 TUBE_N = 256
 METRIC = "Mcell-updates/s per RK4 step"
 UNIT = "Mcell-updates/s"
+
+
+def alg_bytes_mixed(ndim):
+    """The same for the mixed form: stage states in float (4 B), the base
+    state as a float high/low pair (8 B), accumulator and backgrounds in
+    double: stage 0 reads Un_hi,B writes U2,Acc (16P+8B bytes); stages 1-2
+    read Us,Un_hi+lo,Acc,B write Us+1,Acc (32P+8B); stage 3 reads U4,Acc,B
+    writes Un+1 hi+lo (20P+8B) -> 100P+32B bytes (2D: 728, 3D: 960)."""
+    P, B = 2 + 2 * ndim, 2 + ndim
+    return 100 * P + 32 * B
 
 
 def alg_bytes_per_cell_step(ndim):
@@ -107,20 +121,20 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(self.samples)}
 
 
-def make_case(N, seed=1):
+def make_case(N, seed=1, precision=0):
     from smaug_b200 import ic, params as P
     w, pos, dx = ic.orszag_tang(N, noise=1e-3, seed=seed)
     p = P.make_params(ndim=2, n=(N + 4, N + 4, 1), dx=dx, courant=0.3, dtmax=1.0,
-                      integrator=P.INT_RK4)
+                      integrator=P.INT_RK4, precision=precision)
     return p, w, pos
 
 
-def make_tube(N, seed=1):
+def make_tube(N, seed=1, precision=0):
     """3D stratified atmosphere, N^3 interior cells, 2 x 2 x 6 Mm (dim 0 vertical)."""
     from smaug_b200 import ic, params as P
     w, pos, dx = ic.stratified(nz=N, nx=N, ny=N, seed=seed)
     p = P.make_params(ndim=3, n=(N + 4, N + 4, N + 4), dx=dx, courant=0.3, dtmax=1.0,
-                      integrator=P.INT_RK4, g=(-274.0, 0.0, 0.0),
+                      integrator=P.INT_RK4, g=(-274.0, 0.0, 0.0), precision=precision,
                       boundtype=(P.BC_CONTCD4, P.BC_PERIODIC, P.BC_PERIODIC),
                       driver=P.DRIVER_GAUSS, drv_amp=200.0, drv_period=30.0,
                       drv_x0=(0.1e6, 1.0e6, 1.0e6), drv_sigma=(0.2e6, 0.2e6, 0.2e6))
@@ -130,12 +144,13 @@ def make_tube(N, seed=1):
 def workload(args, seed=1):
     """(params, w, pos, interior cells, description) of the selected workload."""
     N = args.n
+    prec = 1 if args.precision == "mixed" else 0
     if args.workload == "tube":
-        p, w, pos = make_tube(N, seed)
+        p, w, pos = make_tube(N, seed, prec)
         return p, w, pos, N ** 3, ("3D stratified atmosphere %dx%dx%d (+2 ghost layers), 2x2x6 Mm, "
                                    "contcd4 vertical / periodic horizontal, gravity, Gaussian "
                                    "driver, hyperdiffusion, CFL 0.3, FP64, classical RK4" % (N, N, N))
-    p, w, pos = make_case(N, seed)
+    p, w, pos = make_case(N, seed, prec)
     return p, w, pos, N * N, ("2D Orszag-Tang %dx%d (+2 ghost layers), periodic, "
                               "hyperdiffusion, CFL 0.3, FP64, classical RK4" % (N, N))
 
@@ -233,15 +248,20 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="ot", choices=["ot", "tube"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--n", type=int, default=None)
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--ref-sample", type=int, default=512)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ref-gpu", action="store_true")
+    ap.add_argument("--no-mixed", dest="mixed", action="store_false",
+                    help="skip the mixed precision measurement")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.n is None:
         args.n = TUBE_N if args.workload == "tube" else WORKLOAD_N
+    if args.precision == "mixed":
+        args.mixed = False
     ws, rank, local = dist_setup(args)
     if args.impl == "reference":
         reference_arm(args, ws, rank)
@@ -293,6 +313,7 @@ def main():
     ms_max = float(t.item())
     value = ncell_int * args.steps * ws / (ms_max / 1e3) / 1e6
     launches = 4 * args.steps
+    ref_state = eng.state() if args.mixed else None
 
     # e2e: host buffers through the C ABI, pinned memory, copies in the timed region
     nvar = p.nvar
@@ -320,6 +341,53 @@ def main():
     d2h = nvar * p.ncells * 8
     eng.close()
 
+    # the mixed precision form on the same workload: same warm-up and timed
+    # steps, its state compared with the FP64 state after the same steps
+    mixed = None
+    if args.mixed:
+        from smaug_b200 import params as P
+        pm = P.SmaugParams.from_buffer_copy(p)
+        pm.precision = P.PREC_MIXED
+        em = engine.Engine(pm, w, pos)
+        em.set_stream(stream.cuda_stream)
+        em.step_async(args.warmup)
+        em.sync()
+        torch.cuda.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        m0 = torch.cuda.Event(enable_timing=True)
+        m1 = torch.cuda.Event(enable_timing=True)
+        m0.record(stream)
+        em.step_async(args.steps)
+        m1.record(stream)
+        torch.cuda.synchronize()
+        em.sync()
+        barrier()
+        mms = m0.elapsed_time(m1)
+        tm = torch.tensor([mms], dtype=torch.float64, device="cuda")
+        if ws > 1:
+            import torch.distributed as dist
+            dist.all_reduce(tm, op=dist.ReduceOp.MAX)
+        mms = float(tm.item())
+        mst = em.state()
+        em.close()
+        nevo = 2 + 2 * p.ndim
+        errs = []
+        for f in range(nevo):
+            d = float(np.sqrt(np.sum((mst[f] - ref_state[f]) ** 2)))
+            n = float(np.sqrt(np.sum(ref_state[f] ** 2)))
+            errs.append(d / n if n > 0 else d)
+        mval = ncell_int * args.steps * ws / (mms / 1e3) / 1e6
+        mbytes = alg_bytes_mixed(p.ndim)
+        peak_m, _ = peaks()
+        mach = mbytes * ncell_int * args.steps / (mms / 1e3) / 1e9
+        mixed = {"value": mval, "unit": UNIT, "ms_per_step": mms / args.steps,
+                 "speedup_vs_fp64": mval / value, "dtype": "f32 storage + hyperdiffusion, f64 rest",
+                 "rel_l2_vs_fp64": {"steps": args.warmup + args.steps, "max": max(errs),
+                                    "per_field": errs},
+                 "roofline": {"bound": "hbm", "achieved": mach, "peak": peak_m, "unit": "GB/s",
+                              "frac": mach / peak_m, "alg_bytes_per_cell_step": mbytes}}
+
     if rank == 0:
         peak, pk_kind = peaks()
         achieved = alg_bytes * ncell_int * args.steps / (ms / 1e3) / 1e9
@@ -344,6 +412,7 @@ def main():
                          "alg_bytes_per_cell_step": alg_bytes,
                          "note": "stage kernel; FP64 arithmetic, not HBM, limits this form"},
             "clocks": clk.summary(),
+            "mixed": mixed,
         }
         if ws == 1 and not args.no_cpu_baseline and args.workload == "ot":
             os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))

@@ -61,6 +61,11 @@ extern "C" {
 
 /* precision forms */
 #define SMAUG_PREC_FP64 0
+/* mixed: perturbation fields stored in float (the base state as a float
+   high/low pair), backgrounds, fluxes, pressure recovery, CFL speeds and the
+   RK4 accumulator in double, hyperdiffusion arithmetic in float; the host
+   interface (get/set state, .out files) stays FP64 */
+#define SMAUG_PREC_MIXED 1
 
 /* Fill model of the outer layer of the padded array from which the
    reference's right-biased hyperviscosity is computed.  hyperdifvisc1r_parallel

@@ -1,27 +1,58 @@
-"""Build the engine shared library (sm_100a) in-tree: smaug_b200/libsmaug_b200.so."""
+"""Build the engine shared library (sm_100a) in-tree: smaug_b200/libsmaug_b200.so.
+
+The translation units (the 2D and 3D stage kernels, the engine host code and
+the file formats) compile to objects in parallel under smaug_b200/_build/,
+then nvcc links them.  An object is rebuilt when its source or one of the
+headers under csrc/ or include/ is newer than it.
+"""
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libsmaug_b200.so")
-SRCS = [os.path.join(HERE, "csrc", f) for f in ("engine.cu", "host_io.cpp")]
-DEPS = SRCS + [os.path.join(HERE, "csrc", f) for f in sorted(os.listdir(os.path.join(HERE, "csrc")))
-               if f.endswith((".h", ".cuh"))] + [os.path.join(ROOT, "include", "smaug_b200.h")]
+OBJDIR = os.path.join(HERE, "_build")
+CSRC = os.path.join(HERE, "csrc")
+SRCS = [os.path.join(CSRC, f) for f in ("engine.cu", "stage2d.cu", "stage3d.cu", "host_io.cpp")]
+HEADERS = [os.path.join(CSRC, f) for f in sorted(os.listdir(CSRC)) if f.endswith((".h", ".cuh"))] + [
+    os.path.join(ROOT, "include", "smaug_b200.h")]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2"]
 
 
-def build(force=False, verbose=False, extra=()):
-    if (not force and os.path.exists(LIB)
-            and os.path.getmtime(LIB) >= max(os.path.getmtime(d) for d in DEPS)):
-        return LIB
-    cmd = (["nvcc"] + ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
-                              "-Xcompiler", "-O2", "-shared", "-o", LIB] + list(extra) + SRCS
-           + ["-lcudart"])
+def _obj(src):
+    return os.path.join(OBJDIR, os.path.basename(src) + ".o")
+
+
+def _stale(target, deps):
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def _compile(src, extra, verbose):
+    cmd = ["nvcc"] + ARCH + FLAGS + list(extra) + ["-c", "-o", _obj(src), src]
     if verbose:
         print(" ".join(cmd), flush=True)
     subprocess.check_call(cmd)
+
+
+def build(force=False, verbose=False, extra=()):
+    os.makedirs(OBJDIR, exist_ok=True)
+    todo = [s for s in SRCS if force or _stale(_obj(s), [s] + HEADERS)]
+    if todo:
+        with ThreadPoolExecutor(max_workers=len(todo)) as ex:
+            for f in [ex.submit(_compile, s, extra, verbose) for s in todo]:
+                f.result()
+    objs = [_obj(s) for s in SRCS]
+    if force or todo or _stale(LIB, objs):
+        cmd = ["nvcc"] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.check_call(cmd)
     return LIB
 
 

@@ -31,8 +31,9 @@
 
 #include "../../include/smaug_b200.h"
 #include "engine_internal.h"
+#include "kernels.cuh"
 
-#define SMAUG_VERSION_STRING "smaug_b200 0.2 (sm_100a, fp64, 2D+3D)"
+#define SMAUG_VERSION_STRING "smaug_b200 0.3 (sm_100a, fp64 + mixed, 2D+3D)"
 
 namespace smaug {
 
@@ -62,159 +63,8 @@ const char* last_error() { return g_err.c_str(); }
   } while (0)
 
 // ---------------------------------------------------------------------------
-// kernel parameters
-// ---------------------------------------------------------------------------
-constexpr int TX = 32;             // tile width (x, fastest)
-constexpr int TY = 8;              // tile height
-constexpr int HALO = 3;            // stencil radius of the hyperdiffusion windows
-constexpr int RX = TX + 2 * HALO;  // staged region
-constexpr int RY = TY + 2 * HALO;
-constexpr int RC = RX * RY;
-constexpr int NTHREADS = TX * TY;
-constexpr int NF2 = 10;            // 2D fields: 6 evolved + 4 background
-
-// 2D field ids (include/iotypes.h:209-216)
-enum { RHO = 0, M1 = 1, M2 = 2, EN = 3, B1 = 4, B2 = 5, EB = 6, RHOB = 7, BB1 = 8, BB2 = 9 };
-
-struct KParams {
-  int n0, n1, n2;   // n2 = 1 in 2D
-  long ncell;
-  int bt[3];        // boundtype[dim][0] (upper) -- gradient edge zeroing
-  int bc[3];        // ghost-fill type per dim
-  double gamma, courant, dtmax;
-  double dx[3];
-  double g[3];
-  double chyp[SMAUG_MAXVAR];
-  int moddton, hyperdif, has_bg, has_grav, driver;
-  double drv_amp, drv_period, drv_x0[3], drv_sigma[3];
-};
-
-struct KBufs {
-  const double* uin;   // [6][ncell] stage input (ghosts valid)
-  const double* un;    // [6][ncell] RK base state
-  double* uout;        // [6][ncell] stage output
-  double* acc;         // [6][ncell] RK accumulator
-  const double* bg;    // [4][ncell] energyb, rhob, b1b, b2b
-  const double* delx[3];
-  const double* pos[3];
-  const int* padsrc[3];
-  const double* cmax_in;          // [3]
-  unsigned long long* cmax_out;   // [3] (double bits, atomicMax)
-  unsigned long long* cmax_clear; // [3] zeroed for the launch after next
-  const double* dt_prev;          // dt of the previous step
-  double* dt_new;                 // dt of this step (written by stage 0)
-  const double* t_prev;
-  double* t_new;
-  int* flags;
-  int mode;   // SMAUG_INT_EULER / SMAUG_INT_RK4
-  int stage;  // 0..3
-};
-
-// ---------------------------------------------------------------------------
-// device helpers
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ double dmax0(double m, double v) { return (v > m) ? v : m; }
-
-// dt rule, src/iosmaug.c:541-616 (a rejected candidate keeps the previous dt,
-// see the oracle's dt_rule for why)
-__device__ double device_dt(const KParams& P, const double* cmax, double dt_prev, int nd) {
-  if (P.moddton != 1) return dt_prev;
-  double courantmax = 1.0e-12;
-  double cm = cmax[nd - 1];
-  for (int d = 0; d < nd; d++) {
-    double t = cm / P.dx[d];
-    if (t > courantmax) courantmax = t;
-  }
-  double dttemp = P.courant / courantmax;
-  if (dttemp > 1.0e-12 && dttemp < P.dtmax) return dttemp;
-  return dt_prev;
-}
-
-// computec3 (src/dervfields.cu:241-309), 2D, fast speed along `dir`
-__device__ __forceinline__ double cfast2(double gamma, double rho, double m1, double m2, double e,
-                                         double b1, double b2, double eb, double rhob, double bb1,
-                                         double bb2, int dir) {
-  double m2s = m1 * m1 + m2 * m2;
-  double b2s = b1 * b1 + b2 * b2;
-  double bbb = bb1 * b1 + bb2 * b2;
-  double bb2s = bb1 * bb1 + bb2 * bb2;
-  double rt = rho + rhob;
-  double pk = (gamma - 1) * (e - 0.5 * (m2s / rt) - 0.5 * b2s - bbb);
-  double cs2 = (gamma * (pk + (gamma - 1) * (eb - 0.5 * bb2s))) / rt;
-  double cf = (b2s + bb2s + 2.0 * bbb) / rt + cs2;
-  double bd = (dir == 0) ? (bb1 + b1) : (bb2 + b2);
-  double md = (dir == 0) ? m1 : m2;
-  double cfasti = 0.5 * (cf + sqrt(cf * cf - 4.0 * cs2 * (bd * bd) / rt));
-  return sqrt(cfasti) + fabs(md / rt);
-}
-
-// ghost images of interior index a along a dimension of n cells (the
-// reference's fill of ghost indices from interior sources, per type)
-__device__ __forceinline__ int ghost_images(int a, int n, int type, int* img) {
-  int c = 0;
-  switch (type) {
-    case SMAUG_BC_PERIODIC:
-      if (a == n - 4 || a == n - 3) img[c++] = a - (n - 4);
-      if (a == 2 || a == 3) img[c++] = a + n - 4;
-      break;
-    case SMAUG_BC_CONTCD4:
-      if (a == 4) img[c++] = 0;
-      if (a == 3) img[c++] = 1;
-      if (a == n - 4) img[c++] = n - 2;
-      if (a == n - 5) img[c++] = n - 1;
-      break;
-    case SMAUG_BC_CONT:
-      if (a == 2) { img[c++] = 0; img[c++] = 1; }
-      if (a == n - 3) { img[c++] = n - 2; img[c++] = n - 1; }
-      break;
-    case SMAUG_BC_SYMM:
-      if (a == 3) img[c++] = 0;
-      if (a == 2) img[c++] = 1;
-      if (a == n - 4) img[c++] = n - 1;
-      if (a == n - 3) img[c++] = n - 2;
-      break;
-    default:
-      break;
-  }
-  return c;
-}
-
-// edge zeroing of the gradient operators when boundtype != 0
-// (src/gradops.cu:459-474 for grad3dn, :620-823 for the 2nd-order ones;
-// evaluated for cells whose other coordinates are inside the band, where the
-// reference's precedence-dependent conditions reduce to these sets)
-__device__ __forceinline__ bool zero3dn(int a, int n) {
-  return a == 2 || a == 3 || a == n - 4 || a == n - 3;
-}
-__device__ __forceinline__ bool zero1n(int a, int n) {
-  return a == 1 || a == 2 || a == n - 3 || a == n - 2;
-}
-
-// ---------------------------------------------------------------------------
-// 2D stage kernel
-// ---------------------------------------------------------------------------
-#include "stage2d.cuh"
-
-// ---------------------------------------------------------------------------
-// 3D stage kernel
-// ---------------------------------------------------------------------------
-#include "stage3d.cuh"
-
-// ---------------------------------------------------------------------------
 // auxiliary kernels: ghost fill and CFL maxima of an arbitrary state
 // ---------------------------------------------------------------------------
-// source interior index of a ghost index (inverse of ghost_images)
-__device__ __forceinline__ int ghost_source(int a, int n, int type) {
-  if (a >= 2 && a <= n - 3) return a;
-  switch (type) {
-    case SMAUG_BC_PERIODIC: return (a < 2) ? n - 4 + a : a - n + 4;
-    case SMAUG_BC_CONTCD4: return (a < 2) ? 4 - a : (a == n - 1 ? n - 5 : n - 4);
-    case SMAUG_BC_CONT: return (a < 2) ? 2 : n - 3;
-    case SMAUG_BC_SYMM: return (a < 2) ? 3 - a : 2 * n - 5 - a;
-    default: return a;
-  }
-}
-
 __global__ void ghost_fill2d_kernel(const KParams P, double* u) {
   long c = blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (c >= P.ncell) return;
@@ -285,7 +135,10 @@ struct Engine {
   int nd = 2, nevo = 6, nbg = 4;
   long ncell = 0;
   cudaStream_t stream = nullptr;
-  double* d_u[3] = {nullptr, nullptr, nullptr};
+  bool mix = false;                      // mixed precision form
+  double* d_u[3] = {nullptr, nullptr, nullptr};  // FP64 form: rotating state buffers
+  float* d_h[4] = {nullptr, nullptr, nullptr, nullptr};  // mixed form: float buffers
+  double* d_x64 = nullptr;               // mixed form: FP64 state for host copies
   double* d_acc = nullptr;
   double* d_bg = nullptr;
   double* d_delx[3] = {nullptr, nullptr, nullptr};
@@ -308,10 +161,13 @@ static void free_engine(Engine* e) {
   if (!e) return;
   for (int i = 0; i < 3; i++) {
     cudaFree(e->d_u[i]);
+    cudaFree(e->d_h[i]);
     cudaFree(e->d_delx[i]);
     cudaFree(e->d_pos[i]);
     cudaFree(e->d_pad[i]);
   }
+  cudaFree(e->d_h[3]);
+  cudaFree(e->d_x64);
   cudaFree(e->d_acc);
   cudaFree(e->d_bg);
   cudaFree(e->d_cmax);
@@ -332,8 +188,8 @@ static int validate(const smaug_params_t* p) {
     if (p->n[d] < 8) return set_error(SMAUG_E_INVALID, "n[%d]=%d: need at least 4 interior cells", d, p->n[d]);
   if (p->integrator != SMAUG_INT_EULER && p->integrator != SMAUG_INT_RK4)
     return set_error(SMAUG_E_INVALID, "unknown integrator %d", p->integrator);
-  if (p->precision != SMAUG_PREC_FP64)
-    return set_error(SMAUG_E_UNSUPPORTED, "precision form %d not implemented", p->precision);
+  if (p->precision != SMAUG_PREC_FP64 && p->precision != SMAUG_PREC_MIXED)
+    return set_error(SMAUG_E_INVALID, "unknown precision form %d", p->precision);
   if (p->pad_model != SMAUG_PAD_STRAY && p->pad_model != SMAUG_PAD_ZERO)
     return set_error(SMAUG_E_INVALID, "unknown pad model %d", p->pad_model);
   for (int d = 0; d < p->ndim; d++) {
@@ -484,8 +340,14 @@ static int create(const smaug_params_t* p, const double* w, const double* pos, E
   E_TRY(cudaStreamCreateWithFlags(&e->own_stream, cudaStreamNonBlocking));
   e->stream = e->own_stream;
   size_t evo_bytes = sizeof(double) * e->nevo * nc;
-  for (int i = 0; i < 3; i++) E_TRY(cudaMalloc(&e->d_u[i], evo_bytes));
-  E_TRY(cudaMalloc(&e->d_acc, evo_bytes));
+  e->mix = (p->precision == SMAUG_PREC_MIXED);
+  if (e->mix) {
+    for (int i = 0; i < 4; i++) E_TRY(cudaMalloc(&e->d_h[i], sizeof(float) * e->nevo * nc));
+    E_TRY(cudaMalloc(&e->d_x64, evo_bytes));
+  } else {
+    for (int i = 0; i < 3; i++) E_TRY(cudaMalloc(&e->d_u[i], evo_bytes));
+  }
+  if (p->integrator == SMAUG_INT_RK4) E_TRY(cudaMalloc(&e->d_acc, evo_bytes));
   E_TRY(cudaMalloc(&e->d_bg, sizeof(double) * e->nbg * nc));
   for (int d = 0; d < e->nd; d++) {
     E_TRY(cudaMalloc(&e->d_delx[d], sizeof(double) * p->n[d]));
@@ -500,7 +362,7 @@ static int create(const smaug_params_t* p, const double* w, const double* pos, E
   E_TRY(cudaMalloc(&e->d_dt, sizeof(double) * 2));
   E_TRY(cudaMalloc(&e->d_t, sizeof(double) * 2));
   E_TRY(cudaMalloc(&e->d_flags, sizeof(int)));
-  E_TRY(cudaMemcpy(e->d_u[0], w, evo_bytes, cudaMemcpyHostToDevice));
+  E_TRY(cudaMemcpy(e->mix ? e->d_x64 : e->d_u[0], w, evo_bytes, cudaMemcpyHostToDevice));
   E_TRY(cudaMemcpy(e->d_bg, w + (size_t)e->nevo * nc, sizeof(double) * e->nbg * nc,
                    cudaMemcpyHostToDevice));
   double dt0[2] = {p->dt, p->dt}, t0[2] = {0.0, 0.0};
@@ -514,30 +376,76 @@ static int create(const smaug_params_t* p, const double* w, const double* pos, E
   return SMAUG_OK;
 }
 
-// ghost fill of the current state + CFL maxima into ring slot of the next launch
+// FP64 state of the host interface <-> float high/low pair of the mixed form
+__global__ void split_kernel(const double* x, float* hi, float* lo, long n) {
+  long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double v = x[i];
+  const float h = (float)v;
+  hi[i] = h;
+  lo[i] = (float)(v - (double)h);
+}
+__global__ void join_kernel(const float* hi, const float* lo, double* x, long n) {
+  long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  x[i] = (double)hi[i] + (double)lo[i];
+}
+
+// the float pair holding the current base state (mixed form)
+static float* base_hi(Engine* e) { return e->d_h[2 * e->cur]; }
+static float* base_lo(Engine* e) { return e->d_h[2 * e->cur + 1]; }
+
+// FP64 view of the current state: the state itself (FP64 form) or the
+// conversion buffer filled from the high/low pair (mixed form)
+static int current_fp64(Engine* e, double** out) {
+  if (!e->mix) {
+    *out = e->d_u[e->cur];
+    return SMAUG_OK;
+  }
+  const long n = (long)e->nevo * e->ncell;
+  join_kernel<<<(unsigned)((n + 255) / 256), 256, 0, e->stream>>>(base_hi(e), base_lo(e), e->d_x64, n);
+  CUDA_TRY(cudaGetLastError());
+  *out = e->d_x64;
+  return SMAUG_OK;
+}
+
+// ghost fill of the state just set (the FP64 buffer) + CFL maxima into the
+// ring slot of the next launch; the mixed form then splits it into its pair
 static int reset_derived(Engine* e) {
   const int bs = 256;
   long nb = (e->ncell + bs - 1) / bs;
+  double* u = e->mix ? e->d_x64 : e->d_u[e->cur];
   if (e->nd == 3)
-    ghost_fill3d_kernel<<<(unsigned)nb, bs, 0, e->stream>>>(e->K, e->d_u[e->cur]);
+    ghost_fill3d_kernel<<<(unsigned)nb, bs, 0, e->stream>>>(e->K, u);
   else
-    ghost_fill2d_kernel<<<(unsigned)nb, bs, 0, e->stream>>>(e->K, e->d_u[e->cur]);
+    ghost_fill2d_kernel<<<(unsigned)nb, bs, 0, e->stream>>>(e->K, u);
   CUDA_TRY(cudaGetLastError());
   CUDA_TRY(cudaMemsetAsync(e->d_cmax, 0, sizeof(unsigned long long) * 9, e->stream));
   unsigned long long* slot = e->d_cmax + 3 * (e->stage_count % 3);
   if (e->nd == 3)
-    cmax3d_kernel<<<(unsigned)nb, bs, 0, e->stream>>>(e->K, e->d_u[e->cur], e->d_bg, slot);
+    cmax3d_kernel<<<(unsigned)nb, bs, 0, e->stream>>>(e->K, u, e->d_bg, slot);
   else
-    cmax2d_kernel<<<(unsigned)nb, bs, 0, e->stream>>>(e->K, e->d_u[e->cur], e->d_bg, slot);
+    cmax2d_kernel<<<(unsigned)nb, bs, 0, e->stream>>>(e->K, u, e->d_bg, slot);
   CUDA_TRY(cudaGetLastError());
+  if (e->mix) {
+    const long n = (long)e->nevo * e->ncell;
+    split_kernel<<<(unsigned)((n + bs - 1) / bs), bs, 0, e->stream>>>(u, base_hi(e), base_lo(e), n);
+    CUDA_TRY(cudaGetLastError());
+  }
   return SMAUG_OK;
 }
 
-static int launch_stage(Engine* e, int mode, int stage, const double* uin, const double* un, double* uout) {
+// one stage launch; uin/un/uout are the FP64 buffers or the float buffers
+// of the mixed form (un_lo / uout_lo: low parts where a base state is read
+// or written)
+static int launch_stage(Engine* e, int mode, int stage, const void* uin, const void* un,
+                        const float* un_lo, void* uout, float* uout_lo) {
   KBufs B{};
   B.uin = uin;
   B.un = un;
+  B.un_lo = un_lo;
   B.uout = uout;
+  B.uout_lo = uout_lo;
   B.acc = e->d_acc;
   B.bg = e->d_bg;
   for (int d = 0; d < 3; d++) {
@@ -556,17 +464,10 @@ static int launch_stage(Engine* e, int mode, int stage, const double* uin, const
   B.flags = e->d_flags;
   B.mode = mode;
   B.stage = stage;
-  if (e->nd == 3) {
-    if (mode == SMAUG_INT_EULER)
-      CUDA_TRY(launch_stage3d<SMAUG_INT_EULER>(e->K, B, e->stream));
-    else
-      CUDA_TRY(launch_stage3d<SMAUG_INT_RK4>(e->K, B, e->stream));
-  } else {
-    if (mode == SMAUG_INT_EULER)
-      CUDA_TRY(launch_stage2d<SMAUG_INT_EULER>(e->K, B, e->stream));
-    else
-      CUDA_TRY(launch_stage2d<SMAUG_INT_RK4>(e->K, B, e->stream));
-  }
+  if (e->nd == 3)
+    CUDA_TRY(launch_stage3d_any(mode, e->mix, e->K, B, e->stream));
+  else
+    CUDA_TRY(launch_stage2d_any(mode, e->mix, e->K, B, e->stream));
   e->stage_count++;
   return SMAUG_OK;
 }
@@ -586,18 +487,36 @@ static int sync_check(Engine* e) {
 static int enqueue_steps(Engine* e, int nsteps) {
   for (int s = 0; s < nsteps; s++) {
     int rc;
-    if (e->P.integrator == SMAUG_INT_EULER) {
+    if (e->mix) {
+      if (e->P.integrator == SMAUG_INT_EULER) {
+        // base-state pairs (h0,h1) and (h2,h3) alternate
+        int nxt = 1 - e->cur;
+        rc = launch_stage(e, SMAUG_INT_EULER, 0, base_hi(e), base_hi(e), base_lo(e),
+                          e->d_h[2 * nxt], e->d_h[2 * nxt + 1]);
+        if (rc) return rc;
+        e->cur = nxt;
+      } else {
+        // base state in (h0,h1); stage states in h2, h3
+        float* hi = e->d_h[0];
+        float* lo = e->d_h[1];
+        if ((rc = launch_stage(e, SMAUG_INT_RK4, 0, hi, hi, lo, e->d_h[2], nullptr))) return rc;
+        if ((rc = launch_stage(e, SMAUG_INT_RK4, 1, e->d_h[2], hi, lo, e->d_h[3], nullptr))) return rc;
+        if ((rc = launch_stage(e, SMAUG_INT_RK4, 2, e->d_h[3], hi, lo, e->d_h[2], nullptr))) return rc;
+        if ((rc = launch_stage(e, SMAUG_INT_RK4, 3, e->d_h[2], hi, lo, hi, lo))) return rc;
+      }
+    } else if (e->P.integrator == SMAUG_INT_EULER) {
       int nxt = (e->cur + 1) % 3;
-      rc = launch_stage(e, SMAUG_INT_EULER, 0, e->d_u[e->cur], e->d_u[e->cur], e->d_u[nxt]);
+      rc = launch_stage(e, SMAUG_INT_EULER, 0, e->d_u[e->cur], e->d_u[e->cur], nullptr,
+                        e->d_u[nxt], nullptr);
       if (rc) return rc;
       e->cur = nxt;
     } else {
       int a = (e->cur + 1) % 3, b = (e->cur + 2) % 3;
       double* un = e->d_u[e->cur];
-      if ((rc = launch_stage(e, SMAUG_INT_RK4, 0, un, un, e->d_u[a]))) return rc;
-      if ((rc = launch_stage(e, SMAUG_INT_RK4, 1, e->d_u[a], un, e->d_u[b]))) return rc;
-      if ((rc = launch_stage(e, SMAUG_INT_RK4, 2, e->d_u[b], un, e->d_u[a]))) return rc;
-      if ((rc = launch_stage(e, SMAUG_INT_RK4, 3, e->d_u[a], un, un))) return rc;
+      if ((rc = launch_stage(e, SMAUG_INT_RK4, 0, un, un, nullptr, e->d_u[a], nullptr))) return rc;
+      if ((rc = launch_stage(e, SMAUG_INT_RK4, 1, e->d_u[a], un, nullptr, e->d_u[b], nullptr))) return rc;
+      if ((rc = launch_stage(e, SMAUG_INT_RK4, 2, e->d_u[b], un, nullptr, e->d_u[a], nullptr))) return rc;
+      if ((rc = launch_stage(e, SMAUG_INT_RK4, 3, e->d_u[a], un, nullptr, un, nullptr))) return rc;
     }
     e->parity = 1 - e->parity;
     e->it++;
@@ -700,7 +619,11 @@ extern "C" int smaug_get_state(smaug_handle_t h, double* w) {
   if (!h || !w) return smaug::set_error(SMAUG_E_INVALID, "null argument");
   Engine* e = H(h);
   CUDA_TRY(cudaStreamSynchronize(e->stream));
-  CUDA_TRY(cudaMemcpy(w, e->d_u[e->cur], sizeof(double) * e->nevo * e->ncell, cudaMemcpyDeviceToHost));
+  double* u = nullptr;
+  int rc = smaug::current_fp64(e, &u);
+  if (rc) return rc;
+  CUDA_TRY(cudaMemcpyAsync(w, u, sizeof(double) * e->nevo * e->ncell, cudaMemcpyDeviceToHost, e->stream));
+  CUDA_TRY(cudaStreamSynchronize(e->stream));
   CUDA_TRY(cudaMemcpy(w + (size_t)e->nevo * e->ncell, e->d_bg, sizeof(double) * e->nbg * e->ncell,
                       cudaMemcpyDeviceToHost));
   return SMAUG_OK;
@@ -711,7 +634,8 @@ extern "C" int smaug_set_state(smaug_handle_t h, const double* w) {
   if (!h || !w) return smaug::set_error(SMAUG_E_INVALID, "null argument");
   Engine* e = H(h);
   CUDA_TRY(cudaStreamSynchronize(e->stream));
-  CUDA_TRY(cudaMemcpy(e->d_u[e->cur], w, sizeof(double) * e->nevo * e->ncell, cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpyAsync(e->mix ? e->d_x64 : e->d_u[e->cur], w, sizeof(double) * e->nevo * e->ncell,
+                           cudaMemcpyHostToDevice, e->stream));
   int rc = smaug::reset_derived(e);
   if (rc) return rc;
   CUDA_TRY(cudaStreamSynchronize(e->stream));
@@ -836,6 +760,8 @@ extern "C" int smaug_euler_step_noalloc(const smaug_params_t* p, const double* w
   if (rc) return rc;
   if (!w_in || !w_out || !delx || !dt) return set_error(SMAUG_E_INVALID, "null argument");
   if (p->ndim != 2) return set_error(SMAUG_E_UNSUPPORTED, "the allocation-free step is 2D only");
+  if (p->precision != SMAUG_PREC_FP64)
+    return set_error(SMAUG_E_UNSUPPORTED, "the allocation-free step is FP64 only");
   if (w_in == w_out) return set_error(SMAUG_E_INVALID, "w_in and w_out must not alias");
   if (p->n[0] > NOALLOC_MAXN || p->n[1] > NOALLOC_MAXN)
     return set_error(SMAUG_E_UNSUPPORTED,
@@ -909,7 +835,7 @@ extern "C" int smaug_euler_step_noalloc(const smaug_params_t* p, const double* w
   B.mode = SMAUG_INT_EULER;
   B.stage = 0;
   CUDA_TRY(stage2d_set_attributes());
-  CUDA_TRY(launch_stage2d<SMAUG_INT_EULER>(K, B, st));
+  CUDA_TRY(launch_stage2d_any(SMAUG_INT_EULER, false, K, B, st));
   // background fields are constant: carry them to the output
   CUDA_TRY(cudaMemcpyAsync(w_out + 6 * nc, bg, sizeof(double) * 4 * nc, cudaMemcpyDeviceToDevice, st));
   int hflags = 0;

@@ -1,0 +1,223 @@
+// kernels.cuh -- definitions shared by the engine's translation units:
+// tile constants, field numbering, kernel parameter blocks, the precision
+// forms and the device helpers of the stage kernels (engine.cu, stage2d.cu,
+// stage3d.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cmath>
+
+#include "../../include/smaug_b200.h"
+
+namespace smaug {
+
+// ---------------------------------------------------------------------------
+// kernel parameters
+// ---------------------------------------------------------------------------
+constexpr int TX = 32;             // tile width (x, fastest)
+constexpr int TY = 8;              // tile height
+constexpr int HALO = 3;            // stencil radius of the hyperdiffusion windows
+constexpr int RX = TX + 2 * HALO;  // staged region
+constexpr int RY = TY + 2 * HALO;
+constexpr int RC = RX * RY;
+constexpr int NTHREADS = TX * TY;
+
+// 2D field ids (include/iotypes.h:209-216)
+enum { RHO = 0, M1 = 1, M2 = 2, EN = 3, B1 = 4, B2 = 5, EB = 6, RHOB = 7, BB1 = 8, BB2 = 9 };
+
+struct KParams {
+  int n0, n1, n2;   // n2 = 1 in 2D
+  long ncell;
+  int bt[3];        // boundtype[dim][0] (upper) -- gradient edge zeroing
+  int bc[3];        // ghost-fill type per dim
+  double gamma, courant, dtmax;
+  double dx[3];
+  double g[3];
+  double chyp[SMAUG_MAXVAR];
+  int moddton, hyperdif, has_bg, has_grav, driver;
+  double drv_amp, drv_period, drv_x0[3], drv_sigma[3];
+};
+
+struct KBufs {
+  const void* uin;     // [P][ncell] stage input, ghosts valid (double; float in the mixed form)
+  const void* un;      // [P][ncell] RK base state (double; its high part in the mixed form)
+  const float* un_lo;  // mixed form: low part of the base state
+  void* uout;          // [P][ncell] stage output
+  float* uout_lo;      // mixed form: low part, written where the output is a base state
+  double* acc;         // [P][ncell] RK accumulator (FP64 in both forms)
+  const double* bg;    // [B][ncell] background fields (FP64 in both forms)
+  const double* delx[3];
+  const double* pos[3];
+  const int* padsrc[3];
+  const double* cmax_in;          // [3]
+  unsigned long long* cmax_out;   // [3] (double bits, atomicMax)
+  unsigned long long* cmax_clear; // [3] zeroed for the launch after next
+  const double* dt_prev;          // dt of the previous step
+  double* dt_new;                 // dt of this step (written by stage 0)
+  const double* t_prev;
+  double* t_new;
+  int* flags;
+  int mode;   // SMAUG_INT_EULER / SMAUG_INT_RK4
+  int stage;  // 0..3
+};
+
+// storage and hyperdiffusion arithmetic types of a precision form
+template <bool MIX>
+struct Form {
+  using S = double;  // perturbation storage
+  using H = double;  // hyperdiffusion arithmetic
+};
+template <>
+struct Form<true> {
+  using S = float;
+  using H = float;
+};
+
+// ---------------------------------------------------------------------------
+// device helpers
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double dmax0(double m, double v) { return (v > m) ? v : m; }
+template <typename T>
+__device__ __forceinline__ T hmax0(T m, T v) { return (v > m) ? v : m; }
+
+// dt rule, src/iosmaug.c:541-616 (a rejected candidate keeps the previous dt,
+// see the oracle's dt_rule for why)
+__device__ __forceinline__ double device_dt(const KParams& P, const double* cmax, double dt_prev, int nd) {
+  if (P.moddton != 1) return dt_prev;
+  double courantmax = 1.0e-12;
+  double cm = cmax[nd - 1];
+  for (int d = 0; d < nd; d++) {
+    double t = cm / P.dx[d];
+    if (t > courantmax) courantmax = t;
+  }
+  double dttemp = P.courant / courantmax;
+  if (dttemp > 1.0e-12 && dttemp < P.dtmax) return dttemp;
+  return dt_prev;
+}
+
+// computec3 (src/dervfields.cu:241-309), 2D, fast speed along `dir`
+__device__ __forceinline__ double cfast2(double gamma, double rho, double m1, double m2, double e,
+                                         double b1, double b2, double eb, double rhob, double bb1,
+                                         double bb2, int dir) {
+  double m2s = m1 * m1 + m2 * m2;
+  double b2s = b1 * b1 + b2 * b2;
+  double bbb = bb1 * b1 + bb2 * b2;
+  double bb2s = bb1 * bb1 + bb2 * bb2;
+  double rt = rho + rhob;
+  double pk = (gamma - 1) * (e - 0.5 * (m2s / rt) - 0.5 * b2s - bbb);
+  double cs2 = (gamma * (pk + (gamma - 1) * (eb - 0.5 * bb2s))) / rt;
+  double cf = (b2s + bb2s + 2.0 * bbb) / rt + cs2;
+  double bd = (dir == 0) ? (bb1 + b1) : (bb2 + b2);
+  double md = (dir == 0) ? m1 : m2;
+  double cfasti = 0.5 * (cf + sqrt(cf * cf - 4.0 * cs2 * (bd * bd) / rt));
+  return sqrt(cfasti) + fabs(md / rt);
+}
+
+// ghost images of interior index a along a dimension of n cells (the
+// reference's fill of ghost indices from interior sources, per type)
+__device__ __forceinline__ int ghost_images(int a, int n, int type, int* img) {
+  int c = 0;
+  switch (type) {
+    case SMAUG_BC_PERIODIC:
+      if (a == n - 4 || a == n - 3) img[c++] = a - (n - 4);
+      if (a == 2 || a == 3) img[c++] = a + n - 4;
+      break;
+    case SMAUG_BC_CONTCD4:
+      if (a == 4) img[c++] = 0;
+      if (a == 3) img[c++] = 1;
+      if (a == n - 4) img[c++] = n - 2;
+      if (a == n - 5) img[c++] = n - 1;
+      break;
+    case SMAUG_BC_CONT:
+      if (a == 2) { img[c++] = 0; img[c++] = 1; }
+      if (a == n - 3) { img[c++] = n - 2; img[c++] = n - 1; }
+      break;
+    case SMAUG_BC_SYMM:
+      if (a == 3) img[c++] = 0;
+      if (a == 2) img[c++] = 1;
+      if (a == n - 4) img[c++] = n - 1;
+      if (a == n - 3) img[c++] = n - 2;
+      break;
+    default:
+      break;
+  }
+  return c;
+}
+
+// edge zeroing of the gradient operators when boundtype != 0
+// (src/gradops.cu:459-474 for grad3dn, :620-823 for the 2nd-order ones;
+// evaluated for cells whose other coordinates are inside the band, where the
+// reference's precedence-dependent conditions reduce to these sets)
+__device__ __forceinline__ bool zero3dn(int a, int n) {
+  return a == 2 || a == 3 || a == n - 4 || a == n - 3;
+}
+__device__ __forceinline__ bool zero1n(int a, int n) {
+  return a == 1 || a == 2 || a == n - 3 || a == n - 2;
+}
+
+// 3D field ids of the evolved buffer and of the background buffer
+enum { R3 = 0, M3 = 1, E3 = 4, B3 = 5 };            // m_c = M3 + c, b_c = B3 + c
+enum { GEB = 0, GRB = 1, GBB = 2 };                 // bb_c = GBB + c
+
+// computec3 (src/dervfields.cu:241-309), 3D, fast speed along `dir`
+__device__ __forceinline__ double cfast3(double gamma, const double* s, const double* g, int dir) {
+  const double m2s = s[1] * s[1] + s[2] * s[2] + s[3] * s[3];
+  const double b2s = s[5] * s[5] + s[6] * s[6] + s[7] * s[7];
+  const double bbb = g[2] * s[5] + g[3] * s[6] + g[4] * s[7];
+  const double bb2s = g[2] * g[2] + g[3] * g[3] + g[4] * g[4];
+  const double rt = s[0] + g[1];
+  const double pk = (gamma - 1) * (s[4] - 0.5 * (m2s / rt) - 0.5 * b2s - bbb);
+  const double cs2 = (gamma * (pk + (gamma - 1) * (g[0] - 0.5 * bb2s))) / rt;
+  const double cf = (b2s + bb2s + 2.0 * bbb) / rt + cs2;
+  const double bd = g[2 + dir] + s[5 + dir];
+  const double cfasti = 0.5 * (cf + sqrt(cf * cf - 4.0 * cs2 * (bd * bd) / rt));
+  return sqrt(cfasti) + fabs(s[1 + dir] / rt);
+}
+
+// 4th-order centred derivative along the stride s (grad3dn, src/gradops.cu:437-602)
+__device__ __forceinline__ double d4(const double* a, int l, int s, double rdl2) {
+  return ((8.0 * (a[l + s] - a[l - s]) + (a[l - 2 * s] - a[l + 2 * s])) * (1.0 / 6.0)) * rdl2;
+}
+
+// base state of a field value (the RK4 base / the Euler input) in double
+template <bool MIX>
+__device__ __forceinline__ double base_value(const KBufs& B, long idx) {
+  if (MIX)
+    return (double)static_cast<const float*>(B.un)[idx] + (double)B.un_lo[idx];
+  return static_cast<const double*>(B.un)[idx];
+}
+
+// store of one stage result; a base state keeps a float high/low pair in the
+// mixed form
+template <bool MIX>
+__device__ __forceinline__ void store_value(const KBufs& B, long idx, double v, bool is_base) {
+  if (MIX) {
+    const float hi = (float)v;
+    static_cast<float*>(B.uout)[idx] = hi;
+    if (is_base) B.uout_lo[idx] = (float)(v - (double)hi);
+  } else {
+    static_cast<double*>(B.uout)[idx] = v;
+  }
+}
+
+// source interior index of a ghost index (inverse of ghost_images)
+__device__ __forceinline__ int ghost_source(int a, int n, int type) {
+  if (a >= 2 && a <= n - 3) return a;
+  switch (type) {
+    case SMAUG_BC_PERIODIC: return (a < 2) ? n - 4 + a : a - n + 4;
+    case SMAUG_BC_CONTCD4: return (a < 2) ? 4 - a : (a == n - 1 ? n - 5 : n - 4);
+    case SMAUG_BC_CONT: return (a < 2) ? 2 : n - 3;
+    case SMAUG_BC_SYMM: return (a < 2) ? 3 - a : 2 * n - 5 - a;
+    default: return a;
+  }
+}
+
+
+// stage launches (stage2d.cu, stage3d.cu): mode = SMAUG_INT_EULER / _RK4,
+// mix = the mixed precision form
+cudaError_t launch_stage2d_any(int mode, bool mix, const KParams& K, const KBufs& B, cudaStream_t st);
+cudaError_t launch_stage3d_any(int mode, bool mix, const KParams& K, const KBufs& B, cudaStream_t st);
+cudaError_t stage2d_set_attributes();
+cudaError_t stage3d_set_attributes();
+
+}  // namespace smaug

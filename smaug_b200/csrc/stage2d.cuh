@@ -1,4 +1,4 @@
-// stage2d.cuh -- fused 2D stage kernel (FP64), included by engine.cu.
+// stage2d.cuh -- fused 2D stage kernel, included by stage2d.cu.
 //
 // One launch evaluates the reference's whole spatial operator for a 32x8
 // tile of interior cells and writes the stage result, its ghost images and
@@ -8,8 +8,19 @@
 // width replaced by multiplications with per-cell / per-line reciprocals
 // (agreement with the reference stays at rounding level, ~1e-16 relative).
 //
-// Shared memory (doubles): NS state fields x RC, 1/rho_t x RC, the tile's
-// cell widths and their reciprocals, then one union of phase scratch:
+// Two precision forms share the code (template MIX):
+//   FP64   every value and every operation in double;
+//   mixed  perturbation fields stored in float (stage buffers, and the base
+//          state as a float high/low pair), backgrounds in double; fluxes,
+//          the pressure recovery p_t = (g-1)(e - m^2/2rho_t) - ..., the
+//          CFL speeds, the stage sums and the RK4 accumulator in double;
+//          the hyperdiffusion coefficient and sources (q, nu, their
+//          differences) in float, with q itself formed in double.
+//
+// Shared memory: the tile's state (6 perturbation fields in the storage
+// type, the background fields in double) on the tile + 3-cell halo, 1/rho_t,
+// the tile's cell widths and their reciprocals, then one union of phase
+// scratch:
 //   flux phase:  5 flux arrays on the tile +-2 cells along the direction
 //                (+ 2 velocity arrays when background fields are present)
 //   hyperdiffusion phase: q on the tile +-3 along dim / +-1 across,
@@ -21,31 +32,36 @@ namespace s2 {
 constexpr int FSZ = (TX + 4) * TY > TX * (TY + 4) ? (TX + 4) * TY : TX * (TY + 4);
 constexpr int QSZ = RX * (TY + 2) > (TX + 2) * RY ? RX * (TY + 2) : (TX + 2) * RY;
 constexpr int NSZ = TX * (TY + 2) > (TX + 2) * TY ? TX * (TY + 2) : (TX + 2) * TY;
-constexpr int FLUX_SCR = 5 * FSZ;
-constexpr int HYP_SCR = QSZ + 4 * NSZ;
-constexpr int UNION = FLUX_SCR > HYP_SCR ? FLUX_SCR : HYP_SCR;
-template <bool BG>
-__host__ __device__ constexpr int nstate() { return BG ? 10 : 6; }
-template <bool BG>
+template <bool MIX>
+__host__ __device__ constexpr size_t union_bytes() {
+  return (5 * FSZ * sizeof(double)) > (QSZ + 4 * NSZ) * sizeof(typename Form<MIX>::H)
+             ? 5 * FSZ * sizeof(double)
+             : (QSZ + 4 * NSZ) * sizeof(typename Form<MIX>::H);
+}
+template <bool BG, bool MIX>
 __host__ __device__ constexpr size_t smem_bytes() {
-  return sizeof(double) * ((size_t)(nstate<BG>() + 1 + (BG ? 2 : 0)) * RC + 2 * (RX + RY) + UNION);
+  return 6 * RC * sizeof(typename Form<MIX>::S) +
+         sizeof(double) * ((BG ? 6 : 0) * RC + RC + 2 * (RX + RY)) + union_bytes<MIX>();
 }
 }  // namespace s2
 
-template <bool BG>
+template <bool BG, bool MIX>
 struct T2 {
-  double* S;     // [NS][RC] state
+  using ST = typename Form<MIX>::S;
+  ST* S;         // [6][RC] perturbation state
+  double* G;     // [4][RC] background fields (BG only)
   double* R;     // [RC] 1/rho_t
   double* V;     // [2][RC] velocities (BG only)
   double* dl0;   // [RX] widths along x of the region columns
   double* dl1;   // [RY]
   double* rd0;   // [RX] reciprocals
   double* rd1;   // [RY]
-  double* U;     // union scratch
+  void* U;       // union scratch
   int x0, y0;
-  __device__ __forceinline__ double s(int f, int l) const {
-    if (BG) return S[f * RC + l];
-    return (f < 6) ? S[f * RC + l] : (f == RHOB ? 0.0 : 0.0);
+  // field f of the reference numbering at region cell l, in double
+  __device__ __forceinline__ double v(int f, int l) const {
+    if (f < 6) return (double)S[f * RC + l];
+    return BG ? G[(f - 6) * RC + l] : 0.0;
   }
 };
 
@@ -55,15 +71,15 @@ struct T2 {
 //   F_m_c = v_D m_c + delta_cD p_t - (B'_c Bb_D + Bb_c B'_D) - B'_c B'_D
 //   F_e   = v_D (e + p_t + e_b) - (B'_D (Bb.m) + Bb_D (B'.m) + B'_D (B'.m)) / rho_t
 //   F_B_c = v_D (B'_c + Bb_c) - v_c (B'_D + Bb_D)
-template <bool BG, int D>
-__device__ __forceinline__ void flux_at(const T2<BG>& T, double gamma, int l, double* F) {
-  const double rho = T.S[RHO * RC + l], m1 = T.S[M1 * RC + l], m2 = T.S[M2 * RC + l];
-  const double e = T.S[EN * RC + l], b1 = T.S[B1 * RC + l], b2 = T.S[B2 * RC + l];
+template <bool BG, bool MIX, int D>
+__device__ __forceinline__ void flux_at(const T2<BG, MIX>& T, double gamma, int l, double* F) {
+  const double m1 = T.v(M1, l), m2 = T.v(M2, l);
+  const double e = T.v(EN, l), b1 = T.v(B1, l), b2 = T.v(B2, l);
   double eb = 0, bb1 = 0, bb2 = 0;
   if (BG) {
-    eb = T.S[EB * RC + l];
-    bb1 = T.S[BB1 * RC + l];
-    bb2 = T.S[BB2 * RC + l];
+    eb = T.v(EB, l);
+    bb1 = T.v(BB1, l);
+    bb2 = T.v(BB2, l);
   }
   const double r = T.R[l];
   const double md = D == 0 ? m1 : m2;
@@ -86,56 +102,54 @@ __device__ __forceinline__ void flux_at(const T2<BG>& T, double gamma, int l, do
     F[4] = vd * (b1 + bb1) - (m1 * r) * (b2 + bb2);
 }
 
-// 4th-order centred derivative along the stride s (grad3dn, src/gradops.cu:437-602)
-__device__ __forceinline__ double d4(const double* a, int l, int s, double rdl2) {
-  return ((8.0 * (a[l + s] - a[l - s]) + (a[l - 2 * s] - a[l + 2 * s])) * (1.0 / 6.0)) * rdl2;
-}
-
-// q of a hyperdiffusion pass at region cell l (src/hyperdifvisc1r.cu:1225-1253)
-template <bool BG, int KIND, int COMP>
-__device__ __forceinline__ double hq_at(const T2<BG>& T, int l) {
-  if (KIND == 0) return T.S[RHO * RC + l];
+// q of a hyperdiffusion pass at region cell l (src/hyperdifvisc1r.cu:1225-1253),
+// formed in double
+template <bool BG, bool MIX, int KIND, int COMP>
+__device__ __forceinline__ double hq_at(const T2<BG, MIX>& T, int l) {
+  if (KIND == 0) return T.v(RHO, l);
   if (KIND == 1) {
-    const double m1 = T.S[M1 * RC + l], m2 = T.S[M2 * RC + l];
-    const double b1 = T.S[B1 * RC + l], b2 = T.S[B2 * RC + l];
-    return T.S[EN * RC + l] - 0.5 * ((b1 * b1 + b2 * b2) + (m1 * m1 + m2 * m2) * T.R[l]);
+    const double m1 = T.v(M1, l), m2 = T.v(M2, l);
+    const double b1 = T.v(B1, l), b2 = T.v(B2, l);
+    return T.v(EN, l) - 0.5 * ((b1 * b1 + b2 * b2) + (m1 * m1 + m2 * m2) * T.R[l]);
   }
-  if (KIND == 2) return T.S[(M1 + COMP) * RC + l] * T.R[l];
-  return T.S[(B1 + COMP) * RC + l];
+  if (KIND == 2) return T.v(M1 + COMP, l) * T.R[l];
+  return T.v(B1 + COMP, l);
 }
 
 // the same q from global memory (stray pad source cell)
-template <int KIND, int COMP>
-__device__ __forceinline__ double hq_global(const KBufs& B, long nc, long c) {
-  const double rho = B.uin[0 * nc + c], rhob = B.bg[1 * nc + c];
+template <typename ST, int KIND, int COMP>
+__device__ __forceinline__ double hq_global(const ST* u, const double* bg, long nc, long c) {
+  const double rho = u[0 * nc + c], rhob = bg[1 * nc + c];
   if (KIND == 0) return rho;
   const double r = 1.0 / (rho + rhob);
   if (KIND == 1) {
-    const double m1 = B.uin[1 * nc + c], m2 = B.uin[2 * nc + c];
-    const double b1 = B.uin[4 * nc + c], b2 = B.uin[5 * nc + c];
-    return B.uin[3 * nc + c] - 0.5 * ((b1 * b1 + b2 * b2) + (m1 * m1 + m2 * m2) * r);
+    const double m1 = u[1 * nc + c], m2 = u[2 * nc + c];
+    const double b1 = u[4 * nc + c], b2 = u[5 * nc + c];
+    return (double)u[3 * nc + c] - 0.5 * ((b1 * b1 + b2 * b2) + (m1 * m1 + m2 * m2) * r);
   }
-  if (KIND == 2) return B.uin[(1 + COMP) * nc + c] * r;
-  return B.uin[(4 + COMP) * nc + c];
+  if (KIND == 2) return (double)u[(1 + COMP) * nc + c] * r;
+  return u[(4 + COMP) * nc + c];
 }
 
 // One hyperdiffusion pass: field kind (0 rho, 1 energy, 2 momentum, 3 B),
 // component COMP, direction DIM (src/iosmaug.c:696-810 order).
-template <bool BG, int KIND, int COMP, int DIM>
-__device__ __forceinline__ void hyper_pass(const T2<BG>& T, const KParams& P, const KBufs& B,
+template <bool BG, bool MIX, int KIND, int COMP, int DIM>
+__device__ __forceinline__ void hyper_pass(const T2<BG, MIX>& T, const KParams& P, const KBufs& B,
                                            int tid, bool active, int lxo, int lyo, int gi, int gj,
                                            double dt, double* out) {
+  using HT = typename Form<MIX>::H;
+  using ST = typename Form<MIX>::S;
   constexpr int SX = (DIM == 0), SY = (DIM == 1);
   constexpr int QFIELD = (KIND == 0) ? RHO : (KIND == 1) ? EN : (KIND == 2) ? M1 + COMP : B1 + COMP;
   constexpr bool CROSS = (KIND == 2 && COMP != DIM) || (KIND == 3);
   const int n0 = P.n0, n1 = P.n1;
   const int nd = DIM == 0 ? n0 : n1;
   const long nc = P.ncell;
-  double* Q = T.U;                  // region-indexed (RX stride) q
-  double* NR = T.U + s2::QSZ;       // nu_r, region-indexed rows/cols of the nu area
-  double* NL = NR + s2::NSZ;
-  double* C3 = NL + s2::NSZ;
-  double* C4 = C3 + s2::NSZ;
+  HT* Q = static_cast<HT*>(T.U);    // region-indexed (RX stride) q
+  HT* NR = Q + s2::QSZ;             // nu_r, region-indexed rows/cols of the nu area
+  HT* NL = NR + s2::NSZ;
+  HT* C3 = NL + s2::NSZ;
+  HT* C4 = C3 + s2::NSZ;
   // nu area: tile along DIM, +-1 across; indexed (ly - oyN) * exN + (lx - oxN)
   constexpr int exN = (DIM == 0) ? TX : TX + 2, eyN = (DIM == 0) ? TY + 2 : TY;
   constexpr int oxN = (DIM == 0) ? HALO : HALO - 1, oyN = (DIM == 0) ? HALO - 1 : HALO;
@@ -155,43 +169,43 @@ __device__ __forceinline__ void hyper_pass(const T2<BG>& T, const KParams& P, co
     double q = 0.0;
     if (tr >= 0 && tr < ntr) {
       if (a >= 0 && a < nd) {
-        q = hq_at<BG, KIND, COMP>(T, ly * RX + lx);
+        q = hq_at<BG, MIX, KIND, COMP>(T, ly * RX + lx);
       } else if (a == -1) {
-        q = hq_at<BG, KIND, COMP>(T, (ly + 6 * SY) * RX + lx + 6 * SX);
+        q = hq_at<BG, MIX, KIND, COMP>(T, (ly + 6 * SY) * RX + lx + 6 * SX);
       } else if (a == nd) {
         const int src = B.padsrc[DIM][tr];
-        if (src >= 0) q = hq_global<KIND, COMP>(B, nc, src);
+        if (src >= 0) q = hq_global<ST, KIND, COMP>(static_cast<const ST*>(B.uin), B.bg, nc, src);
       }
     }
-    Q[r] = q;
+    Q[r] = (HT)q;
   }
   __syncthreads();
   // (B) nu_r, nu_l (hyperdifvisc2-4): third differences D3 over faces
   // i-2..i+1, first differences D1 over faces i-3..i+2
-  const double coef = B.cmax_in[DIM] * P.chyp[QFIELD];
+  const HT coef = (HT)(B.cmax_in[DIM] * P.chyp[QFIELD]);
   for (int r = tid; r < exN * eyN; r += NTHREADS) {
     const int lx = oxN + r % exN, ly = oyN + r / exN;
     const int ci = T.x0 - HALO + lx, cj = T.y0 - HALO + ly;
-    double nur = 0.0, nul = 0.0;
+    HT nur = 0, nul = 0;
     if (ci >= 2 && ci <= n0 - 3 && cj >= 2 && cj <= n1 - 3) {
       const int q0 = qi(lx, ly);
       constexpr int st = DIM == 0 ? 1 : exQ;
-      double q[7];
+      HT q[7];
 #pragma unroll
       for (int s = 0; s < 7; s++) q[s] = Q[q0 + (s - 3) * st];
-      double d1[6], d3[4];
+      HT d1[6], d3[4];
 #pragma unroll
       for (int k = 0; k < 6; k++) d1[k] = fabs(q[k + 1] - q[k]);
 #pragma unroll
-      for (int k = 0; k < 4; k++) d3[k] = fabs(3.0 * (q[k + 2] - q[k + 1]) - (q[k + 3] - q[k]));
-      double t4r = 0, t5r = 0, t4l = 0, t5l = 0;
-      t4r = dmax0(dmax0(dmax0(t4r, d3[1]), d3[2]), d3[3]);
-      t4l = dmax0(dmax0(dmax0(t4l, d3[0]), d3[1]), d3[2]);
+      for (int k = 0; k < 4; k++) d3[k] = fabs((HT)3 * (q[k + 2] - q[k + 1]) - (q[k + 3] - q[k]));
+      HT t4r = 0, t5r = 0, t4l = 0, t5l = 0;
+      t4r = hmax0(hmax0(hmax0(t4r, d3[1]), d3[2]), d3[3]);
+      t4l = hmax0(hmax0(hmax0(t4l, d3[0]), d3[1]), d3[2]);
 #pragma unroll
-      for (int k = 1; k < 6; k++) t5r = dmax0(t5r, d1[k]);
+      for (int k = 1; k < 6; k++) t5r = hmax0(t5r, d1[k]);
 #pragma unroll
-      for (int k = 0; k < 5; k++) t5l = dmax0(t5l, d1[k]);
-      const double c = (DIM == 0 ? T.dl0[lx] : T.dl1[ly]) * coef;
+      for (int k = 0; k < 5; k++) t5l = hmax0(t5l, d1[k]);
+      const HT c = (HT)(DIM == 0 ? T.dl0[lx] : T.dl1[ly]) * coef;
       if (t5r > 0) nur = c * t4r / t5r;
       if (t5l > 0) nul = c * t4l / t5l;
     }
@@ -204,24 +218,24 @@ __device__ __forceinline__ void hyper_pass(const T2<BG>& T, const KParams& P, co
     for (int r = tid; r < exN * eyN; r += NTHREADS) {
       const int lx = oxN + r % exN, ly = oyN + r / exN;
       const int ci = T.x0 - HALO + lx, cj = T.y0 - HALO + ly;
-      double c3 = 0.0, c4 = 0.0;
+      HT c3 = 0, c4 = 0;
       if (ci > 0 && ci < n0 - 1 && cj > 0 && cj < n1 - 1) {
         const int a = DIM == 0 ? ci : cj;
         const int q0 = qi(lx, ly);
         constexpr int st = DIM == 0 ? 1 : exQ;
         // grad13n along DIM of q
-        double g = ((Q[q0 + st] - Q[q0 - st]) * (DIM == 0 ? T.rd0[lx] : T.rd1[ly])) * 0.5;
+        HT g = ((Q[q0 + st] - Q[q0 - st]) * (HT)(DIM == 0 ? T.rd0[lx] : T.rd1[ly])) * (HT)0.5;
         if ((P.bt[DIM] != 0) && zero1n(a, nd)) g = 0;
-        const double nsum = NR[r] + NL[r];
+        const HT nsum = NR[r] + NL[r];
         const int l = ly * RX + lx;
         if (KIND == 2) {
-          const double tau = (g * nsum) * 0.25;
-          c3 = (T.S[RHO * RC + l] + (BG ? T.S[RHOB * RC + l] : 0.0)) * tau;
-          c4 = tau * T.S[(M1 + DIM) * RC + l];
+          const HT tau = (g * nsum) * (HT)0.25;
+          c3 = (HT)(T.v(RHO, l) + T.v(RHOB, l)) * tau;
+          c4 = tau * (HT)T.v(M1 + DIM, l);
         } else {
-          const double t3 = (g * nsum) * 0.5;
+          const HT t3 = (g * nsum) * (HT)0.5;
           c3 = t3;
-          c4 = t3 * T.S[(B1 + DIM) * RC + l];
+          c4 = t3 * (HT)T.v(B1 + DIM, l);
         }
       }
       C3[r] = c3;
@@ -235,31 +249,29 @@ __device__ __forceinline__ void hyper_pass(const T2<BG>& T, const KParams& P, co
     const int q0 = qi(lxo, lyo);
     constexpr int st = DIM == 0 ? 1 : exQ;
     const int nidx = ni(lxo, lyo);
-    const double nur = NR[nidx], nul = NL[nidx];
-    const double rdl = DIM == 0 ? T.rd0[lxo] : T.rd1[lyo];
-    const double qc = Q[q0], qp = Q[q0 + st], qm = Q[q0 - st];
-    double gr = (qp - qc) * rdl;   // grad1r3n
-    double gl = (qc - qm) * rdl;   // grad1l3n
+    const HT nur = NR[nidx], nul = NL[nidx];
+    const HT rdl = (HT)(DIM == 0 ? T.rd0[lxo] : T.rd1[lyo]);
+    const HT qc = Q[q0], qp = Q[q0 + st], qm = Q[q0 - st];
+    HT gr = (qp - qc) * rdl;   // grad1r3n
+    HT gl = (qc - qm) * rdl;   // grad1l3n
     if ((P.bt[DIM] != 0) && zero1n(a, nd)) { gr = 0; gl = 0; }
     const int l = lyo * RX + lxo;
     constexpr int SL = SX + SY * RX;  // region stride along DIM
     if (KIND == 0) {
-      out[RHO] = out[RHO] + dt * (nur * gr - nul * gl) * rdl;
+      out[RHO] = out[RHO] + dt * (double)((nur * gr - nul * gl) * rdl);
     } else if (KIND == 1) {
-      out[EN] = out[EN] + dt * (nur * gr - nul * gl) * rdl;
+      out[EN] = out[EN] + dt * (double)((nur * gr - nul * gl) * rdl);
     } else if (KIND == 2) {
       // hyperdifmomsource1-3a (src/hyperdifmomsource1.cu:17-511), ii0 = COMP
-      const double rb0 = BG ? T.S[RHOB * RC + l] : 0.0;
-      const double rbm = BG ? T.S[RHOB * RC + l - SL] : 0.0;
-      const double rbp = BG ? T.S[RHOB * RC + l + SL] : 0.0;
-      const double r0 = T.S[RHO * RC + l];
-      const double t2 = (r0 + rb0 + T.S[RHO * RC + l - SL] + rbm) * 0.5;
-      const double t3 = (r0 + rb0 + T.S[RHO * RC + l + SL] + rbp) * 0.5;
-      const double mf = T.S[(M1 + COMP) * RC + l];
-      const double t5 = (mf + T.S[(M1 + COMP) * RC + l - SL]) * 0.5;
-      const double t6 = (mf + T.S[(M1 + COMP) * RC + l + SL]) * 0.5;
-      const double dm = ((t3 * nur * gr - t2 * nul * gl) * rdl) * 0.5;
-      const double de = ((t6 * nur * gr - t5 * nul * gl) * rdl) * 0.5;
+      const double rb0 = T.v(RHOB, l), rbm = T.v(RHOB, l - SL), rbp = T.v(RHOB, l + SL);
+      const double r0 = T.v(RHO, l);
+      const HT t2 = (HT)((r0 + rb0 + T.v(RHO, l - SL) + rbm) * 0.5);
+      const HT t3 = (HT)((r0 + rb0 + T.v(RHO, l + SL) + rbp) * 0.5);
+      const double mf = T.v(M1 + COMP, l);
+      const HT t5 = (HT)((mf + T.v(M1 + COMP, l - SL)) * 0.5);
+      const HT t6 = (HT)((mf + T.v(M1 + COMP, l + SL)) * 0.5);
+      const double dm = (double)(((t3 * nur * gr - t2 * nul * gl) * rdl) * (HT)0.5);
+      const double de = (double)(((t6 * nur * gr - t5 * nul * gl) * rdl) * (HT)0.5);
       out[M1 + COMP] = out[M1 + COMP] + dt * dm;
       out[EN] = out[EN] + dt * de;
       if (COMP == DIM) {
@@ -269,27 +281,27 @@ __device__ __forceinline__ void hyper_pass(const T2<BG>& T, const KParams& P, co
         // hyperdifmomsourcene5-6a: d/dx_COMP of (rho_t tau) and (tau m_DIM)
         constexpr int FS = (COMP == 0) ? 1 : exN;  // stride across in the nu area
         const int af = COMP == 0 ? gi : gj;
-        const double rdf = COMP == 0 ? T.rd0[lxo] : T.rd1[lyo];
-        double g7 = ((C3[nidx + FS] - C3[nidx - FS]) * rdf) * 0.5;
-        double g8 = ((C4[nidx + FS] - C4[nidx - FS]) * rdf) * 0.5;
+        const HT rdf = (HT)(COMP == 0 ? T.rd0[lxo] : T.rd1[lyo]);
+        HT g7 = ((C3[nidx + FS] - C3[nidx - FS]) * rdf) * (HT)0.5;
+        HT g8 = ((C4[nidx + FS] - C4[nidx - FS]) * rdf) * (HT)0.5;
         if ((P.bt[COMP] != 0) && zero1n(af, COMP == 0 ? n0 : n1)) { g7 = 0; g8 = 0; }
-        out[M1 + DIM] = out[M1 + DIM] + dt * g7;
-        out[EN] = out[EN] + dt * g8;
+        out[M1 + DIM] = out[M1 + DIM] + dt * (double)g7;
+        out[EN] = out[EN] + dt * (double)g8;
       }
     } else {
       // B component COMP diffused along DIM: hyperdifbsourcene (sb=-1) then
       // hyperdifbsource (sb=+1)
       constexpr int FS = (COMP == 0) ? 1 : exN;
       const int af = COMP == 0 ? gi : gj;
-      const double rdf = COMP == 0 ? T.rd0[lxo] : T.rd1[lyo];
-      double g4 = ((C3[nidx + FS] - C3[nidx - FS]) * rdf) * 0.5;
-      double g6 = ((C4[nidx + FS] - C4[nidx - FS]) * rdf) * 0.5;
+      const HT rdf = (HT)(COMP == 0 ? T.rd0[lxo] : T.rd1[lyo]);
+      HT g4 = ((C3[nidx + FS] - C3[nidx - FS]) * rdf) * (HT)0.5;
+      HT g6 = ((C4[nidx + FS] - C4[nidx - FS]) * rdf) * (HT)0.5;
       if ((P.bt[COMP] != 0) && zero1n(af, COMP == 0 ? n0 : n1)) { g4 = 0; g6 = 0; }
-      out[B1 + DIM] = out[B1 + DIM] - dt * g4;
-      out[EN] = out[EN] - dt * g6;
-      const double t2 = (qc + qm) * 0.5, t3 = (qc + qp) * 0.5;
-      const double dB = (gr * nur - gl * nul) * rdl;
-      const double de = (t3 * gr * nur - t2 * gl * nul) * rdl;
+      out[B1 + DIM] = out[B1 + DIM] - dt * (double)g4;
+      out[EN] = out[EN] - dt * (double)g6;
+      const HT t2 = (qc + qm) * (HT)0.5, t3 = (qc + qp) * (HT)0.5;
+      const double dB = (double)((gr * nur - gl * nul) * rdl);
+      const double de = (double)((t3 * gr * nur - t2 * gl * nul) * rdl);
       out[B1 + COMP] = out[B1 + COMP] + dt * dB;
       out[EN] = out[EN] + dt * de;
     }
@@ -297,13 +309,17 @@ __device__ __forceinline__ void hyper_pass(const T2<BG>& T, const KParams& P, co
   __syncthreads();
 }
 
-template <int MODE, bool BG>
+template <int MODE, bool BG, bool MIX>
 __global__ void __launch_bounds__(NTHREADS, 3) stage2d_fast(const KParams P, const KBufs B) {
+  using ST = typename Form<MIX>::S;
   extern __shared__ double smem[];
-  T2<BG> T;
-  constexpr int NS = s2::nstate<BG>();
-  T.S = smem;
-  T.R = smem + NS * RC;
+  T2<BG, MIX> T;
+  unsigned char* sp = reinterpret_cast<unsigned char*>(smem);
+  T.S = reinterpret_cast<ST*>(sp);
+  sp += 6 * RC * sizeof(ST);
+  T.G = reinterpret_cast<double*>(sp);
+  sp += (BG ? 4 * RC : 0) * sizeof(double);
+  T.R = reinterpret_cast<double*>(sp);
   T.V = T.R + RC;
   T.dl0 = T.V + (BG ? 2 * RC : 0);
   T.dl1 = T.dl0 + RX;
@@ -315,6 +331,7 @@ __global__ void __launch_bounds__(NTHREADS, 3) stage2d_fast(const KParams P, con
   T.y0 = 2 + blockIdx.y * TY;
   const int n0 = P.n0, n1 = P.n1;
   const long nc = P.ncell;
+  const ST* uin = static_cast<const ST*>(B.uin);
 
   // ---- stage the tile, 1/rho_t, the metric -------------------------------
   for (int r = tid; r < RC; r += NTHREADS) {
@@ -325,7 +342,7 @@ __global__ void __launch_bounds__(NTHREADS, 3) stage2d_fast(const KParams P, con
     double rho = 0.0, rhob = 1.0;
 #pragma unroll
     for (int f = 0; f < 6; f++) {
-      const double v = in ? __ldg(B.uin + f * nc + c) : 0.0;
+      const ST v = in ? __ldg(uin + f * nc + c) : (ST)0;
       T.S[f * RC + r] = v;
       if (f == 0) rho = v;
     }
@@ -333,7 +350,7 @@ __global__ void __launch_bounds__(NTHREADS, 3) stage2d_fast(const KParams P, con
 #pragma unroll
       for (int f = 0; f < 4; f++) {
         const double v = in ? __ldg(B.bg + f * nc + c) : (f == 1 ? 1.0 : 0.0);
-        T.S[(6 + f) * RC + r] = v;
+        T.G[f * RC + r] = v;
         if (f == 1) rhob = v;
       }
     } else {
@@ -343,8 +360,8 @@ __global__ void __launch_bounds__(NTHREADS, 3) stage2d_fast(const KParams P, con
     const double rinv = 1.0 / (rho + rhob);
     T.R[r] = rinv;
     if (BG) {
-      T.V[r] = T.S[M1 * RC + r] * rinv;
-      T.V[RC + r] = T.S[M2 * RC + r] * rinv;
+      T.V[r] = (double)T.S[M1 * RC + r] * rinv;
+      T.V[RC + r] = (double)T.S[M2 * RC + r] * rinv;
     }
   }
   for (int r = tid; r < RX + RY; r += NTHREADS) {
@@ -382,26 +399,34 @@ __global__ void __launch_bounds__(NTHREADS, 3) stage2d_fast(const KParams P, con
   const int lxo = tx + HALO, lyo = ty + HALO, lo = lyo * RX + lxo;
   const int gi = T.x0 + tx, gj = T.y0 + ty;
   const bool active = gi <= n0 - 3 && gj <= n1 - 3;
+  const long co = active ? (long)gj * n0 + gi : 0;
 
   double out[6];
 #pragma unroll
-  for (int f = 0; f < 6; f++) out[f] = (MODE == SMAUG_INT_EULER) ? T.S[f * RC + lo] : 0.0;
+  for (int f = 0; f < 6; f++) {
+    if (MODE != SMAUG_INT_EULER)
+      out[f] = 0.0;
+    else if (MIX)
+      out[f] = active ? base_value<MIX>(B, f * nc + co) : 0.0;
+    else
+      out[f] = T.v(f, lo);
+  }
 
   // ---- fluxes and divergence (centdiff1 / centdiff2), direction 0 then 1 --
 #pragma unroll
   for (int d = 0; d < 2; d++) {
     const int ex = (d == 0) ? TX + 4 : TX, ey = (d == 0) ? TY : TY + 4;
     const int ox = (d == 0) ? 1 : HALO, oy = (d == 0) ? HALO : 1;
-    double* F = T.U;
+    double* F = static_cast<double*>(T.U);
     for (int r = tid; r < ex * ey; r += NTHREADS) {
       const int lx = ox + r % ex, ly = oy + r / ex;
       const int ci = T.x0 - HALO + lx, cj = T.y0 - HALO + ly;
       double f5[5] = {0, 0, 0, 0, 0};
       if (ci >= 0 && ci < n0 && cj >= 0 && cj < n1) {
         if (d == 0)
-          flux_at<BG, 0>(T, P.gamma, ly * RX + lx, f5);
+          flux_at<BG, MIX, 0>(T, P.gamma, ly * RX + lx, f5);
         else
-          flux_at<BG, 1>(T, P.gamma, ly * RX + lx, f5);
+          flux_at<BG, MIX, 1>(T, P.gamma, ly * RX + lx, f5);
       }
 #pragma unroll
       for (int k = 0; k < 5; k++) F[k * s2::FSZ + r] = f5[k];
@@ -422,7 +447,7 @@ __global__ void __launch_bounds__(NTHREADS, 3) stage2d_fast(const KParams P, con
       }
       if (BG) {
         // addenergyterms_cd2 (src/centdiff2.cu:80-115)
-        const double eb = T.S[EB * RC + lo], bb1 = T.S[BB1 * RC + lo], bb2 = T.S[BB2 * RC + lo];
+        const double eb = T.v(EB, lo), bb1 = T.v(BB1, lo), bb2 = T.v(BB2, lo);
         const double ptb = (P.gamma - 1) * eb - 0.5 * (P.gamma - 2) * (bb1 * bb1 + bb2 * bb2);
         const double* v = T.V + d * RC;
         double gv = d4(v, lo, d == 0 ? 1 : RX, rdl2);
@@ -442,26 +467,22 @@ __global__ void __launch_bounds__(NTHREADS, 3) stage2d_fast(const KParams P, con
 
   // ---- gravity (addgrav_cd2, src/centdiff2.cu:118-154) --------------------
   if (P.has_grav && active) {
-    const double rho = T.S[RHO * RC + lo];
+    const double rho = T.v(RHO, lo);
     out[M1] += dt * P.g[0] * rho;
     out[M2] += dt * P.g[1] * rho;
     const double rr = rho * T.R[lo];
-    out[EN] += (dt * P.g[0] * T.S[M1 * RC + lo]) * rr;
-    out[EN] += (dt * P.g[1] * T.S[M2 * RC + lo]) * rr;
+    out[EN] += (dt * P.g[0] * T.v(M1, lo)) * rr;
+    out[EN] += (dt * P.g[1] * T.v(M2, lo)) * rr;
   }
 
   // ---- hyperdiffusion, in the driver's order -------------------------------
   if (P.hyperdif == 1) {
-    hyper_pass<BG, 0, 0, 0>(T, P, B, tid, active, lxo, lyo, gi, gj, dt, out);
-    hyper_pass<BG, 0, 0, 1>(T, P, B, tid, active, lxo, lyo, gi, gj, dt, out);
-    hyper_pass<BG, 1, 0, 0>(T, P, B, tid, active, lxo, lyo, gi, gj, dt, out);
-    hyper_pass<BG, 1, 0, 1>(T, P, B, tid, active, lxo, lyo, gi, gj, dt, out);
-    hyper_pass<BG, 2, 0, 0>(T, P, B, tid, active, lxo, lyo, gi, gj, dt, out);
-    hyper_pass<BG, 2, 1, 0>(T, P, B, tid, active, lxo, lyo, gi, gj, dt, out);
-    hyper_pass<BG, 2, 0, 1>(T, P, B, tid, active, lxo, lyo, gi, gj, dt, out);
-    hyper_pass<BG, 2, 1, 1>(T, P, B, tid, active, lxo, lyo, gi, gj, dt, out);
-    hyper_pass<BG, 3, 1, 0>(T, P, B, tid, active, lxo, lyo, gi, gj, dt, out);
-    hyper_pass<BG, 3, 0, 1>(T, P, B, tid, active, lxo, lyo, gi, gj, dt, out);
+#define HP(K, C, D) hyper_pass<BG, MIX, K, C, D>(T, P, B, tid, active, lxo, lyo, gi, gj, dt, out)
+    HP(0, 0, 0); HP(0, 0, 1);
+    HP(1, 0, 0); HP(1, 0, 1);
+    HP(2, 0, 0); HP(2, 1, 0); HP(2, 0, 1); HP(2, 1, 1);
+    HP(3, 1, 0); HP(3, 0, 1);
+#undef HP
   }
 
   // ---- user driver (source_parallel + addsourceterms2) ---------------------
@@ -476,8 +497,8 @@ __global__ void __launch_bounds__(NTHREADS, 3) stage2d_fast(const KParams P, con
       const double x = B.pos[1][gj] - P.drv_x0[1];
       v *= exp(-x * x / (P.drv_sigma[1] * P.drv_sigma[1]));
     }
-    const double rhob = BG ? T.S[RHOB * RC + lo] : B.bg[1 * nc + (long)gj * n0 + gi];
-    const double rr = (MODE == SMAUG_INT_EULER) ? out[RHO] : T.S[RHO * RC + lo];
+    const double rhob = BG ? T.v(RHOB, lo) : B.bg[1 * nc + co];
+    const double rr = (MODE == SMAUG_INT_EULER) ? out[RHO] : T.v(RHO, lo);
     out[M1] = out[M1] + dt * v * (rr + rhob);
   }
 
@@ -485,7 +506,7 @@ __global__ void __launch_bounds__(NTHREADS, 3) stage2d_fast(const KParams P, con
   double cm0 = 0.0, cm1 = 0.0;
   if (active) {
     double res[6];
-    const long c = (long)gj * n0 + gi;
+    const bool is_base = (MODE == SMAUG_INT_EULER) || B.stage == 3;
     if (MODE == SMAUG_INT_EULER) {
 #pragma unroll
       for (int f = 0; f < 6; f++) res[f] = out[f];
@@ -496,14 +517,14 @@ __global__ void __launch_bounds__(NTHREADS, 3) stage2d_fast(const KParams P, con
       for (int f = 0; f < 6; f++) {
         const double dl = out[f];
         if (B.stage == 0) {
-          const double u = T.S[f * RC + lo];
-          B.acc[f * nc + c] = u + wgt * dl;
+          const double u = MIX ? base_value<MIX>(B, f * nc + co) : T.v(f, lo);
+          B.acc[f * nc + co] = u + wgt * dl;
           res[f] = u + cst * dl;
         } else if (B.stage < 3) {
-          B.acc[f * nc + c] = B.acc[f * nc + c] + wgt * dl;
-          res[f] = B.un[f * nc + c] + cst * dl;
+          B.acc[f * nc + co] = B.acc[f * nc + co] + wgt * dl;
+          res[f] = base_value<MIX>(B, f * nc + co) + cst * dl;
         } else {
-          res[f] = B.acc[f * nc + c] + wgt * dl;
+          res[f] = B.acc[f * nc + co] + wgt * dl;
         }
       }
     }
@@ -520,10 +541,10 @@ __global__ void __launch_bounds__(NTHREADS, 3) stage2d_fast(const KParams P, con
       for (int a2 = 0; a2 < nx; a2++) {
         const long cc = (long)iy[b] * n0 + ix[a2];
 #pragma unroll
-        for (int f = 0; f < 6; f++) B.uout[f * nc + cc] = res[f];
+        for (int f = 0; f < 6; f++) store_value<MIX>(B, f * nc + cc, res[f], is_base);
         double eb, rb, b1b, b2b;
         if (BG && a2 == 0 && b == 0) {
-          eb = T.S[EB * RC + lo]; rb = T.S[RHOB * RC + lo]; b1b = T.S[BB1 * RC + lo]; b2b = T.S[BB2 * RC + lo];
+          eb = T.v(EB, lo); rb = T.v(RHOB, lo); b1b = T.v(BB1, lo); b2b = T.v(BB2, lo);
         } else {
           eb = B.bg[0 * nc + cc]; rb = B.bg[1 * nc + cc]; b1b = B.bg[2 * nc + cc]; b2b = B.bg[3 * nc + cc];
         }
@@ -551,29 +572,32 @@ __global__ void __launch_bounds__(NTHREADS, 3) stage2d_fast(const KParams P, con
 }
 
 // launch helper: picks the background specialisation
-template <int MODE>
+template <int MODE, bool MIX>
 static cudaError_t launch_stage2d(const KParams& K, const KBufs& B, cudaStream_t st) {
   dim3 block(TX, TY);
   dim3 grid((K.n0 - 4 + TX - 1) / TX, (K.n1 - 4 + TY - 1) / TY);
   if (K.has_bg) {
-    stage2d_fast<MODE, true><<<grid, block, s2::smem_bytes<true>(), st>>>(K, B);
+    stage2d_fast<MODE, true, MIX><<<grid, block, s2::smem_bytes<true, MIX>(), st>>>(K, B);
   } else {
-    stage2d_fast<MODE, false><<<grid, block, s2::smem_bytes<false>(), st>>>(K, B);
+    stage2d_fast<MODE, false, MIX><<<grid, block, s2::smem_bytes<false, MIX>(), st>>>(K, B);
   }
   return cudaGetLastError();
 }
 
-static cudaError_t stage2d_set_attributes() {
+template <int MODE, bool BG, bool MIX>
+static cudaError_t stage2d_attr() {
+  return cudaFuncSetAttribute(stage2d_fast<MODE, BG, MIX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)s2::smem_bytes<BG, MIX>());
+}
+
+cudaError_t stage2d_set_attributes() {
   cudaError_t e;
-  if ((e = cudaFuncSetAttribute(stage2d_fast<SMAUG_INT_EULER, true>,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s2::smem_bytes<true>())))
-    return e;
-  if ((e = cudaFuncSetAttribute(stage2d_fast<SMAUG_INT_EULER, false>,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s2::smem_bytes<false>())))
-    return e;
-  if ((e = cudaFuncSetAttribute(stage2d_fast<SMAUG_INT_RK4, true>,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s2::smem_bytes<true>())))
-    return e;
-  return cudaFuncSetAttribute(stage2d_fast<SMAUG_INT_RK4, false>,
-                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s2::smem_bytes<false>());
+  if ((e = stage2d_attr<SMAUG_INT_EULER, true, false>())) return e;
+  if ((e = stage2d_attr<SMAUG_INT_EULER, false, false>())) return e;
+  if ((e = stage2d_attr<SMAUG_INT_RK4, true, false>())) return e;
+  if ((e = stage2d_attr<SMAUG_INT_RK4, false, false>())) return e;
+  if ((e = stage2d_attr<SMAUG_INT_EULER, true, true>())) return e;
+  if ((e = stage2d_attr<SMAUG_INT_EULER, false, true>())) return e;
+  if ((e = stage2d_attr<SMAUG_INT_RK4, true, true>())) return e;
+  return stage2d_attr<SMAUG_INT_RK4, false, true>();
 }

@@ -1,4 +1,4 @@
-// stage3d.cuh -- fused 3D stage kernel (FP64), included by engine.cu.
+// stage3d.cuh -- fused 3D stage kernel, included by stage3d.cu.
 //
 // One launch evaluates the reference's whole spatial operator (the 3D build,
 // -DUSE_SAC_3D, of src/iosmaug.c:631-835) for an 8x8x4 tile of interior
@@ -16,7 +16,9 @@
 //     one field share one staging of q
 //   user driver, stage combine, ghost images, CFL maxima.
 // Sums per cell are reordered against the reference (per field instead of
-// per dimension); agreement stays at rounding level.
+// per dimension); agreement stays at rounding level.  The mixed precision
+// form (template MIX) is the one of stage2d.cuh: float perturbation storage
+// and hyperdiffusion arithmetic, double everywhere else.
 //
 // The state is read from global memory (L1/L2 resident across the passes of
 // a block); shared memory holds 1/rho_t and q on the tile's 3-cell box,
@@ -42,56 +44,45 @@ constexpr int FA = max3((T0 + 4) * T1 * T2, T0 * (T1 + 4) * T2, T0 * T1 * (T2 + 
 constexpr int NA = max3(T0 * (T1 + 2) * (T2 + 2), (T0 + 2) * T1 * (T2 + 2), (T0 + 2) * (T1 + 2) * T2);
 constexpr int FLUX_SCR = 10 * FA;
 constexpr int HYP_SCR = BC + 4 * NA;
-constexpr int UNION = FLUX_SCR > HYP_SCR ? FLUX_SCR : HYP_SCR;
 constexpr int NMET = 2 * (BX + BY + BZ);
-__host__ __device__ constexpr size_t smem_bytes() { return sizeof(double) * (BC + NMET + UNION); }
+template <bool MIX>
+__host__ __device__ constexpr size_t union_bytes() {
+  return FLUX_SCR * sizeof(double) > HYP_SCR * sizeof(typename Form<MIX>::H)
+             ? FLUX_SCR * sizeof(double)
+             : HYP_SCR * sizeof(typename Form<MIX>::H);
+}
+template <bool MIX>
+__host__ __device__ constexpr size_t smem_bytes() {
+  return sizeof(double) * (BC + NMET) + union_bytes<MIX>();
+}
 __host__ __device__ constexpr int tdim(int d) { return d == 0 ? T0 : (d == 1 ? T1 : T2); }
 __host__ __device__ constexpr int bstride(int d) { return d == 0 ? 1 : (d == 1 ? BS1 : BS2); }
 }  // namespace s3
-
-// 3D field ids of the evolved buffer and of the background buffer
-enum { R3 = 0, M3 = 1, E3 = 4, B3 = 5 };            // m_c = M3 + c, b_c = B3 + c
-enum { GEB = 0, GRB = 1, GBB = 2 };                 // bb_c = GBB + c
 
 struct Box3 {
   double* R;       // [BC] 1/rho_t on the box
   double* dl[3];   // cell widths over the box extent of each axis
   double* rd[3];   // reciprocals
-  double* U;       // union scratch
+  void* U;         // union scratch
   int o[3];        // global coordinate of box index 0 per axis
 };
 
-// computec3 (src/dervfields.cu:241-309), 3D, fast speed along `dir`
-__device__ __forceinline__ double cfast3(double gamma, const double* s, const double* g, int dir) {
-  const double m2s = s[1] * s[1] + s[2] * s[2] + s[3] * s[3];
-  const double b2s = s[5] * s[5] + s[6] * s[6] + s[7] * s[7];
-  const double bbb = g[2] * s[5] + g[3] * s[6] + g[4] * s[7];
-  const double bb2s = g[2] * g[2] + g[3] * g[3] + g[4] * g[4];
-  const double rt = s[0] + g[1];
-  const double pk = (gamma - 1) * (s[4] - 0.5 * (m2s / rt) - 0.5 * b2s - bbb);
-  const double cs2 = (gamma * (pk + (gamma - 1) * (g[0] - 0.5 * bb2s))) / rt;
-  const double cf = (b2s + bb2s + 2.0 * bbb) / rt + cs2;
-  const double bd = g[2 + dir] + s[5 + dir];
-  const double cfasti = 0.5 * (cf + sqrt(cf * cf - 4.0 * cs2 * (bd * bd) / rt));
-  return sqrt(cfasti) + fabs(s[1 + dir] / rt);
-}
-
 // q of a hyperdiffusion field from global memory (src/hyperdifvisc1r.cu:1225-1253)
-template <int KIND, int COMP>
-__device__ __forceinline__ double hq3_global(const KBufs& B, long nc, long c) {
-  const double rho = __ldg(B.uin + c);
+template <typename ST, int KIND, int COMP>
+__device__ __forceinline__ double hq3_global(const ST* u, const KBufs& B, long nc, long c) {
+  const double rho = __ldg(u + c);
   if (KIND == 0) return rho;
-  if (KIND == 3) return __ldg(B.uin + (B3 + COMP) * nc + c);
+  if (KIND == 3) return __ldg(u + (B3 + COMP) * nc + c);
   const double r = 1.0 / (rho + __ldg(B.bg + GRB * nc + c));
-  if (KIND == 2) return __ldg(B.uin + (M3 + COMP) * nc + c) * r;
+  if (KIND == 2) return (double)__ldg(u + (M3 + COMP) * nc + c) * r;
   double m2 = 0, b2 = 0;
 #pragma unroll
   for (int a = 0; a < 3; a++) {
-    const double m = __ldg(B.uin + (M3 + a) * nc + c), b = __ldg(B.uin + (B3 + a) * nc + c);
+    const double m = __ldg(u + (M3 + a) * nc + c), b = __ldg(u + (B3 + a) * nc + c);
     m2 += m * m;
     b2 += b * b;
   }
-  return __ldg(B.uin + E3 * nc + c) - 0.5 * (b2 + m2 * r);
+  return (double)__ldg(u + E3 * nc + c) - 0.5 * (b2 + m2 * r);
 }
 
 // distance of box index l outside the tile range [H, H+T)
@@ -103,9 +94,12 @@ __device__ __forceinline__ int outside(int l, int T) {
 // axes but one, and within 3 on that one.  Pads: index -1 along an axis is
 // the copy of index 5 (bc_hyperdifl), index n the stray tmp6 store of
 // hyperdifvisc1r_parallel (source table B.padsrc).
-template <int KIND, int COMP>
+template <bool MIX, int KIND, int COMP>
 __device__ __forceinline__ void stage_q(const Box3& X, const KParams& P, const KBufs& B, int tid) {
-  double* Q = X.U;
+  using HT = typename Form<MIX>::H;
+  using ST = typename Form<MIX>::S;
+  const ST* u = static_cast<const ST*>(B.uin);
+  HT* Q = static_cast<HT*>(X.U);
   const long nc = P.ncell;
   const int n[3] = {P.n0, P.n1, P.n2};
   for (int r = tid; r < s3::BC; r += s3::NT) {
@@ -122,42 +116,42 @@ __device__ __forceinline__ void stage_q(const Box3& X, const KParams& P, const K
       if (nout == 0) {
         const long c = ((long)g[2] * n[1] + g[1]) * n[0] + g[0];
         if (KIND == 0) {
-          q = __ldg(B.uin + c);
+          q = __ldg(u + c);
         } else if (KIND == 3) {
-          q = __ldg(B.uin + (B3 + COMP) * nc + c);
+          q = __ldg(u + (B3 + COMP) * nc + c);
         } else if (KIND == 2) {
-          q = __ldg(B.uin + (M3 + COMP) * nc + c) * X.R[r];
+          q = (double)__ldg(u + (M3 + COMP) * nc + c) * X.R[r];
         } else {
           double m2 = 0, b2 = 0;
 #pragma unroll
           for (int a = 0; a < 3; a++) {
-            const double m = __ldg(B.uin + (M3 + a) * nc + c), b = __ldg(B.uin + (B3 + a) * nc + c);
+            const double m = __ldg(u + (M3 + a) * nc + c), b = __ldg(u + (B3 + a) * nc + c);
             m2 += m * m;
             b2 += b * b;
           }
-          q = __ldg(B.uin + E3 * nc + c) - 0.5 * (b2 + m2 * X.R[r]);
+          q = (double)__ldg(u + E3 * nc + c) - 0.5 * (b2 + m2 * X.R[r]);
         }
       } else if (nout == 1) {
         if (g[ax] == -1) {
           g[ax] = 5;
           const long c = ((long)g[2] * n[1] + g[1]) * n[0] + g[0];
-          q = hq3_global<KIND, COMP>(B, nc, c);
+          q = hq3_global<ST, KIND, COMP>(u, B, nc, c);
         } else if (g[ax] == n[ax]) {
           // across index of the pad table: the other two coordinates, lower axis fastest
           const int a1 = ax == 0 ? 1 : 0, a2 = ax == 2 ? 1 : 2;
           const int src = B.padsrc[ax][(long)g[a2] * n[a1] + g[a1]];
-          if (src >= 0) q = hq3_global<KIND, COMP>(B, nc, src);
+          if (src >= 0) q = hq3_global<ST, KIND, COMP>(u, B, nc, src);
         }
       }
     }
-    Q[r] = q;
+    Q[r] = (HT)q;
   }
   __syncthreads();
 }
 
 // One hyperdiffusion pass on staged q: field kind (0 rho, 1 energy,
 // 2 momentum, 3 B), component COMP, direction DIM.
-template <int KIND, int COMP, int DIM>
+template <bool MIX, int KIND, int COMP, int DIM>
 __device__ __forceinline__ void hyper_pass3(const Box3& X, const KParams& P, const KBufs& B, int tid,
                                             bool active, const int* lt, const int* gt, double dt,
                                             double* out) {
@@ -172,40 +166,43 @@ __device__ __forceinline__ void hyper_pass3(const Box3& X, const KParams& P, con
   constexpr int G1 = s3::H - ((CROSS && DIM != 1) ? 1 : 0);
   constexpr int G2 = s3::H - ((CROSS && DIM != 2) ? 1 : 0);
   constexpr int NAREA = E0 * E1 * E2;
+  using HT = typename Form<MIX>::H;
+  using ST = typename Form<MIX>::S;
+  const ST* u = static_cast<const ST*>(B.uin);
   const int n[3] = {P.n0, P.n1, P.n2};
   const long nc = P.ncell;
-  const double* Q = X.U;
-  double* NR = X.U + s3::BC;
-  double* NL = NR + s3::NA;
-  double* C3 = NL + s3::NA;
-  double* C4 = C3 + s3::NA;
+  const HT* Q = static_cast<const HT*>(X.U);
+  HT* NR = static_cast<HT*>(X.U) + s3::BC;
+  HT* NL = NR + s3::NA;
+  HT* C3 = NL + s3::NA;
+  HT* C4 = C3 + s3::NA;
   auto aidx = [&](int lx, int ly, int lz) { return ((lz - G2) * E1 + (ly - G1)) * E0 + (lx - G0); };
 
   // (B) nu_r, nu_l (hyperdifvisc2-4)
-  const double coef = B.cmax_in[DIM] * P.chyp[QFIELD];
+  const HT coef = (HT)(B.cmax_in[DIM] * P.chyp[QFIELD]);
   for (int r = tid; r < NAREA; r += s3::NT) {
     const int lx = G0 + r % E0, ly = G1 + (r / E0) % E1, lz = G2 + r / (E0 * E1);
     const int g0 = X.o[0] + lx, g1 = X.o[1] + ly, g2 = X.o[2] + lz;
-    double nur = 0.0, nul = 0.0;
+    HT nur = 0, nul = 0;
     if (g0 >= 2 && g0 <= n[0] - 3 && g1 >= 2 && g1 <= n[1] - 3 && g2 >= 2 && g2 <= n[2] - 3) {
       const int q0 = (lz * s3::BY + ly) * s3::BX + lx;
-      double q[7];
+      HT q[7];
 #pragma unroll
       for (int s = 0; s < 7; s++) q[s] = Q[q0 + (s - 3) * SD];
-      double d1[6], d3[4];
+      HT d1[6], d3[4];
 #pragma unroll
       for (int k = 0; k < 6; k++) d1[k] = fabs(q[k + 1] - q[k]);
 #pragma unroll
-      for (int k = 0; k < 4; k++) d3[k] = fabs(3.0 * (q[k + 2] - q[k + 1]) - (q[k + 3] - q[k]));
-      double t4r = 0, t5r = 0, t4l = 0, t5l = 0;
-      t4r = dmax0(dmax0(dmax0(t4r, d3[1]), d3[2]), d3[3]);
-      t4l = dmax0(dmax0(dmax0(t4l, d3[0]), d3[1]), d3[2]);
+      for (int k = 0; k < 4; k++) d3[k] = fabs((HT)3 * (q[k + 2] - q[k + 1]) - (q[k + 3] - q[k]));
+      HT t4r = 0, t5r = 0, t4l = 0, t5l = 0;
+      t4r = hmax0(hmax0(hmax0(t4r, d3[1]), d3[2]), d3[3]);
+      t4l = hmax0(hmax0(hmax0(t4l, d3[0]), d3[1]), d3[2]);
 #pragma unroll
-      for (int k = 1; k < 6; k++) t5r = dmax0(t5r, d1[k]);
+      for (int k = 1; k < 6; k++) t5r = hmax0(t5r, d1[k]);
 #pragma unroll
-      for (int k = 0; k < 5; k++) t5l = dmax0(t5l, d1[k]);
+      for (int k = 0; k < 5; k++) t5l = hmax0(t5l, d1[k]);
       const int la = DIM == 0 ? lx : (DIM == 1 ? ly : lz);
-      const double c = X.dl[DIM][la] * coef;
+      const HT c = (HT)X.dl[DIM][la] * coef;
       if (t5r > 0) nur = c * t4r / t5r;
       if (t5l > 0) nul = c * t4l / t5l;
     }
@@ -218,23 +215,23 @@ __device__ __forceinline__ void hyper_pass3(const Box3& X, const KParams& P, con
     for (int r = tid; r < NAREA; r += s3::NT) {
       const int lx = G0 + r % E0, ly = G1 + (r / E0) % E1, lz = G2 + r / (E0 * E1);
       const int g[3] = {X.o[0] + lx, X.o[1] + ly, X.o[2] + lz};
-      double c3 = 0.0, c4 = 0.0;
+      HT c3 = 0, c4 = 0;
       if (g[0] > 0 && g[0] < n[0] - 1 && g[1] > 0 && g[1] < n[1] - 1 && g[2] > 0 && g[2] < n[2] - 1) {
         const int q0 = (lz * s3::BY + ly) * s3::BX + lx;
         const int la = DIM == 0 ? lx : (DIM == 1 ? ly : lz);
         // grad13n along DIM of q
-        double gq = ((Q[q0 + SD] - Q[q0 - SD]) * X.rd[DIM][la]) * 0.5;
+        HT gq = ((Q[q0 + SD] - Q[q0 - SD]) * (HT)X.rd[DIM][la]) * (HT)0.5;
         if ((P.bt[DIM] != 0) && zero1n(g[DIM], n[DIM])) gq = 0;
-        const double nsum = NR[r] + NL[r];
+        const HT nsum = NR[r] + NL[r];
         const long c = ((long)g[2] * n[1] + g[1]) * n[0] + g[0];
         if (KIND == 2) {
-          const double tau = (gq * nsum) * 0.25;
-          c3 = (__ldg(B.uin + c) + __ldg(B.bg + GRB * nc + c)) * tau;
-          c4 = tau * __ldg(B.uin + (M3 + DIM) * nc + c);
+          const HT tau = (gq * nsum) * (HT)0.25;
+          c3 = (HT)((double)__ldg(u + c) + __ldg(B.bg + GRB * nc + c)) * tau;
+          c4 = tau * (HT)__ldg(u + (M3 + DIM) * nc + c);
         } else {
-          const double t3 = (gq * nsum) * 0.5;
+          const HT t3 = (gq * nsum) * (HT)0.5;
           c3 = t3;
-          c4 = t3 * __ldg(B.uin + (B3 + DIM) * nc + c);
+          c4 = t3 * (HT)__ldg(u + (B3 + DIM) * nc + c);
         }
       }
       C3[r] = c3;
@@ -247,31 +244,31 @@ __device__ __forceinline__ void hyper_pass3(const Box3& X, const KParams& P, con
     const int la = lt[DIM];
     const int q0 = (lt[2] * s3::BY + lt[1]) * s3::BX + lt[0];
     const int nidx = aidx(lt[0], lt[1], lt[2]);
-    const double nur = NR[nidx], nul = NL[nidx];
-    const double rdl = X.rd[DIM][la];
-    const double qc = Q[q0], qp = Q[q0 + SD], qm = Q[q0 - SD];
-    double gr = (qp - qc) * rdl;  // grad1r3n
-    double gl = (qc - qm) * rdl;  // grad1l3n
+    const HT nur = NR[nidx], nul = NL[nidx];
+    const HT rdl = (HT)X.rd[DIM][la];
+    const HT qc = Q[q0], qp = Q[q0 + SD], qm = Q[q0 - SD];
+    HT gr = (qp - qc) * rdl;  // grad1r3n
+    HT gl = (qc - qm) * rdl;  // grad1l3n
     if ((P.bt[DIM] != 0) && zero1n(gt[DIM], n[DIM])) { gr = 0; gl = 0; }
     if (KIND == 0) {
-      out[R3] = out[R3] + dt * (nur * gr - nul * gl) * rdl;
+      out[R3] = out[R3] + dt * (double)((nur * gr - nul * gl) * rdl);
     } else if (KIND == 1) {
-      out[E3] = out[E3] + dt * (nur * gr - nul * gl) * rdl;
+      out[E3] = out[E3] + dt * (double)((nur * gr - nul * gl) * rdl);
     } else if (KIND == 2) {
       // hyperdifmomsource1-3a (src/hyperdifmomsource1.cu:17-511), ii0 = COMP
       const long c = ((long)gt[2] * n[1] + gt[1]) * n[0] + gt[0];
       const long sd = DIM == 0 ? 1 : (DIM == 1 ? (long)n[0] : (long)n[0] * n[1]);
-      const double* rho = B.uin;
+      const ST* rho = u;
       const double* rb = B.bg + GRB * nc;
-      const double* mf = B.uin + (M3 + COMP) * nc;
-      const double r0 = __ldg(rho + c) + __ldg(rb + c);
-      const double t2 = (r0 + __ldg(rho + c - sd) + __ldg(rb + c - sd)) * 0.5;
-      const double t3 = (r0 + __ldg(rho + c + sd) + __ldg(rb + c + sd)) * 0.5;
+      const ST* mf = u + (M3 + COMP) * nc;
+      const double r0 = (double)__ldg(rho + c) + __ldg(rb + c);
+      const HT t2 = (HT)((r0 + (double)__ldg(rho + c - sd) + __ldg(rb + c - sd)) * 0.5);
+      const HT t3 = (HT)((r0 + (double)__ldg(rho + c + sd) + __ldg(rb + c + sd)) * 0.5);
       const double m0 = __ldg(mf + c);
-      const double t5 = (m0 + __ldg(mf + c - sd)) * 0.5;
-      const double t6 = (m0 + __ldg(mf + c + sd)) * 0.5;
-      const double dm = ((t3 * nur * gr - t2 * nul * gl) * rdl) * 0.5;
-      const double de = ((t6 * nur * gr - t5 * nul * gl) * rdl) * 0.5;
+      const HT t5 = (HT)((m0 + (double)__ldg(mf + c - sd)) * 0.5);
+      const HT t6 = (HT)((m0 + (double)__ldg(mf + c + sd)) * 0.5);
+      const double dm = (double)(((t3 * nur * gr - t2 * nul * gl) * rdl) * (HT)0.5);
+      const double de = (double)(((t6 * nur * gr - t5 * nul * gl) * rdl) * (HT)0.5);
       out[M3 + COMP] = out[M3 + COMP] + dt * dm;
       out[E3] = out[E3] + dt * de;
       if (COMP == DIM) {
@@ -280,26 +277,26 @@ __device__ __forceinline__ void hyper_pass3(const Box3& X, const KParams& P, con
       } else {
         // hyperdifmomsourcene5-6a: d/dx_COMP of (rho_t tau) and (tau m_DIM)
         constexpr int FS = COMP == 0 ? 1 : (COMP == 1 ? E0 : E0 * E1);
-        const double rdf = X.rd[COMP][lt[COMP]];
-        double g7 = ((C3[nidx + FS] - C3[nidx - FS]) * rdf) * 0.5;
-        double g8 = ((C4[nidx + FS] - C4[nidx - FS]) * rdf) * 0.5;
+        const HT rdf = (HT)X.rd[COMP][lt[COMP]];
+        HT g7 = ((C3[nidx + FS] - C3[nidx - FS]) * rdf) * (HT)0.5;
+        HT g8 = ((C4[nidx + FS] - C4[nidx - FS]) * rdf) * (HT)0.5;
         if ((P.bt[COMP] != 0) && zero1n(gt[COMP], n[COMP])) { g7 = 0; g8 = 0; }
-        out[M3 + DIM] = out[M3 + DIM] + dt * g7;
-        out[E3] = out[E3] + dt * g8;
+        out[M3 + DIM] = out[M3 + DIM] + dt * (double)g7;
+        out[E3] = out[E3] + dt * (double)g8;
       }
     } else {
       // B component COMP diffused along DIM: hyperdifbsourcene (sb=-1) then
       // hyperdifbsource (sb=+1)
       constexpr int FS = COMP == 0 ? 1 : (COMP == 1 ? E0 : E0 * E1);
-      const double rdf = X.rd[COMP][lt[COMP]];
-      double g4 = ((C3[nidx + FS] - C3[nidx - FS]) * rdf) * 0.5;
-      double g6 = ((C4[nidx + FS] - C4[nidx - FS]) * rdf) * 0.5;
+      const HT rdf = (HT)X.rd[COMP][lt[COMP]];
+      HT g4 = ((C3[nidx + FS] - C3[nidx - FS]) * rdf) * (HT)0.5;
+      HT g6 = ((C4[nidx + FS] - C4[nidx - FS]) * rdf) * (HT)0.5;
       if ((P.bt[COMP] != 0) && zero1n(gt[COMP], n[COMP])) { g4 = 0; g6 = 0; }
-      out[B3 + DIM] = out[B3 + DIM] - dt * g4;
-      out[E3] = out[E3] - dt * g6;
-      const double t2 = (qc + qm) * 0.5, t3 = (qc + qp) * 0.5;
-      const double dB = (gr * nur - gl * nul) * rdl;
-      const double de = (t3 * gr * nur - t2 * gl * nul) * rdl;
+      out[B3 + DIM] = out[B3 + DIM] - dt * (double)g4;
+      out[E3] = out[E3] - dt * (double)g6;
+      const HT t2 = (qc + qm) * (HT)0.5, t3 = (qc + qp) * (HT)0.5;
+      const double dB = (double)((gr * nur - gl * nul) * rdl);
+      const double de = (double)((t3 * gr * nur - t2 * gl * nul) * rdl);
       out[B3 + COMP] = out[B3 + COMP] + dt * dB;
       out[E3] = out[E3] + dt * de;
     }
@@ -338,7 +335,7 @@ __device__ __forceinline__ void flux3(const double* s, const double* g, double r
 
 // flux phase along D: fluxes on the tile +-2 along D, divergence and the
 // background energy terms at the tile cells
-template <bool BG, int D>
+template <bool BG, bool MIX, int D>
 __device__ __forceinline__ void flux_pass3(const Box3& X, const KParams& P, const KBufs& B, int tid,
                                            bool active, const int* lt, const int* gt, double dt,
                                            const double* gc, double* out) {
@@ -346,9 +343,11 @@ __device__ __forceinline__ void flux_pass3(const Box3& X, const KParams& P, cons
   constexpr int G0 = s3::H - (D == 0 ? 2 : 0), G1 = s3::H - (D == 1 ? 2 : 0), G2 = s3::H - (D == 2 ? 2 : 0);
   constexpr int NAREA = E0 * E1 * E2;
   constexpr int FS = D == 0 ? 1 : (D == 1 ? E0 : E0 * E1);
+  using ST = typename Form<MIX>::S;
+  const ST* u = static_cast<const ST*>(B.uin);
   const int n[3] = {P.n0, P.n1, P.n2};
   const long nc = P.ncell;
-  double* F = X.U;
+  double* F = static_cast<double*>(X.U);
   for (int r = tid; r < NAREA; r += s3::NT) {
     const int lx = G0 + r % E0, ly = G1 + (r / E0) % E1, lz = G2 + r / (E0 * E1);
     const int g0 = X.o[0] + lx, g1 = X.o[1] + ly, g2 = X.o[2] + lz;
@@ -357,7 +356,7 @@ __device__ __forceinline__ void flux_pass3(const Box3& X, const KParams& P, cons
       const long c = ((long)g2 * n[1] + g1) * n[0] + g0;
       double s[8], g[5] = {0, 0, 0, 0, 0};
 #pragma unroll
-      for (int k = 0; k < 8; k++) s[k] = __ldg(B.uin + k * nc + c);
+      for (int k = 0; k < 8; k++) s[k] = __ldg(u + k * nc + c);
       if (BG) {
 #pragma unroll
         for (int k = 0; k < 5; k++) g[k] = __ldg(B.bg + k * nc + c);
@@ -403,8 +402,10 @@ __device__ __forceinline__ void flux_pass3(const Box3& X, const KParams& P, cons
   __syncthreads();
 }
 
-template <int MODE, bool BG>
+template <int MODE, bool BG, bool MIX>
 __global__ void __launch_bounds__(s3::NT, 3) stage3d_fast(const KParams P, const KBufs B) {
+  using ST = typename Form<MIX>::S;
+  const ST* u = static_cast<const ST*>(B.uin);
   extern __shared__ double smem[];
   Box3 X;
   X.R = smem;
@@ -430,7 +431,7 @@ __global__ void __launch_bounds__(s3::NT, 3) stage3d_fast(const KParams P, const
     double rinv = 1.0;
     if (g0 >= 0 && g0 < n[0] && g1 >= 0 && g1 < n[1] && g2 >= 0 && g2 < n[2]) {
       const long c = ((long)g2 * n[1] + g1) * n[0] + g0;
-      rinv = 1.0 / (__ldg(B.uin + c) + __ldg(B.bg + GRB * nc + c));
+      rinv = 1.0 / ((double)__ldg(u + c) + __ldg(B.bg + GRB * nc + c));
     }
     X.R[r] = rinv;
   }
@@ -468,17 +469,24 @@ __global__ void __launch_bounds__(s3::NT, 3) stage3d_fast(const KParams P, const
 
   double sc[8], gc[5] = {0, 0, 0, 0, 0};
 #pragma unroll
-  for (int f = 0; f < 8; f++) sc[f] = active ? __ldg(B.uin + f * nc + co) : 0.0;
+  for (int f = 0; f < 8; f++) sc[f] = active ? (double)__ldg(u + f * nc + co) : 0.0;
 #pragma unroll
   for (int f = 0; f < 5; f++) gc[f] = active ? __ldg(B.bg + f * nc + co) : 0.0;
   double out[8];
 #pragma unroll
-  for (int f = 0; f < 8; f++) out[f] = (MODE == SMAUG_INT_EULER) ? sc[f] : 0.0;
+  for (int f = 0; f < 8; f++) {
+    if (MODE != SMAUG_INT_EULER)
+      out[f] = 0.0;
+    else if (MIX)
+      out[f] = active ? base_value<MIX>(B, f * nc + co) : 0.0;
+    else
+      out[f] = sc[f];
+  }
 
   // ---- fluxes and divergence, direction 0, 1, 2 ----------------------------
-  flux_pass3<BG, 0>(X, P, B, tid, active, lt, gt, dt, gc, out);
-  flux_pass3<BG, 1>(X, P, B, tid, active, lt, gt, dt, gc, out);
-  flux_pass3<BG, 2>(X, P, B, tid, active, lt, gt, dt, gc, out);
+  flux_pass3<BG, MIX, 0>(X, P, B, tid, active, lt, gt, dt, gc, out);
+  flux_pass3<BG, MIX, 1>(X, P, B, tid, active, lt, gt, dt, gc, out);
+  flux_pass3<BG, MIX, 2>(X, P, B, tid, active, lt, gt, dt, gc, out);
 
   // ---- gravity (addgrav_cd2, src/centdiff2.cu:118-154) --------------------
   if (P.has_grav && active) {
@@ -494,23 +502,25 @@ __global__ void __launch_bounds__(s3::NT, 3) stage3d_fast(const KParams P, const
 
   // ---- hyperdiffusion: one q staging per field, then every direction ----
   if (P.hyperdif == 1) {
-#define HP(K, C, D) hyper_pass3<K, C, D>(X, P, B, tid, active, lt, gt, dt, out)
-    stage_q<0, 0>(X, P, B, tid);
+#define HP(K, C, D) hyper_pass3<MIX, K, C, D>(X, P, B, tid, active, lt, gt, dt, out)
+#define SQ(K, C) stage_q<MIX, K, C>(X, P, B, tid)
+    SQ(0, 0);
     HP(0, 0, 0); HP(0, 0, 1); HP(0, 0, 2);
-    stage_q<1, 0>(X, P, B, tid);
+    SQ(1, 0);
     HP(1, 0, 0); HP(1, 0, 1); HP(1, 0, 2);
-    stage_q<2, 0>(X, P, B, tid);
+    SQ(2, 0);
     HP(2, 0, 0); HP(2, 0, 1); HP(2, 0, 2);
-    stage_q<2, 1>(X, P, B, tid);
+    SQ(2, 1);
     HP(2, 1, 0); HP(2, 1, 1); HP(2, 1, 2);
-    stage_q<2, 2>(X, P, B, tid);
+    SQ(2, 2);
     HP(2, 2, 0); HP(2, 2, 1); HP(2, 2, 2);
-    stage_q<3, 0>(X, P, B, tid);
+    SQ(3, 0);
     HP(3, 0, 1); HP(3, 0, 2);
-    stage_q<3, 1>(X, P, B, tid);
+    SQ(3, 1);
     HP(3, 1, 0); HP(3, 1, 2);
-    stage_q<3, 2>(X, P, B, tid);
+    SQ(3, 2);
     HP(3, 2, 0); HP(3, 2, 1);
+#undef SQ
 #undef HP
   }
 
@@ -533,6 +543,7 @@ __global__ void __launch_bounds__(s3::NT, 3) stage3d_fast(const KParams P, const
   double cm[3] = {0.0, 0.0, 0.0};
   if (active) {
     double res[8];
+    const bool is_base = (MODE == SMAUG_INT_EULER) || B.stage == 3;
     if (MODE == SMAUG_INT_EULER) {
 #pragma unroll
       for (int f = 0; f < 8; f++) res[f] = out[f];
@@ -543,11 +554,12 @@ __global__ void __launch_bounds__(s3::NT, 3) stage3d_fast(const KParams P, const
       for (int f = 0; f < 8; f++) {
         const double dl = out[f];
         if (B.stage == 0) {
-          B.acc[f * nc + co] = sc[f] + wgt * dl;
-          res[f] = sc[f] + cst * dl;
+          const double u0 = MIX ? base_value<MIX>(B, f * nc + co) : sc[f];
+          B.acc[f * nc + co] = u0 + wgt * dl;
+          res[f] = u0 + cst * dl;
         } else if (B.stage < 3) {
           B.acc[f * nc + co] = B.acc[f * nc + co] + wgt * dl;
-          res[f] = B.un[f * nc + co] + cst * dl;
+          res[f] = base_value<MIX>(B, f * nc + co) + cst * dl;
         } else {
           res[f] = B.acc[f * nc + co] + wgt * dl;
         }
@@ -569,7 +581,7 @@ __global__ void __launch_bounds__(s3::NT, 3) stage3d_fast(const KParams P, const
         for (int a2 = 0; a2 < nx; a2++) {
           const long cc = ((long)iz[cz] * n[1] + iy[b]) * n[0] + ix[a2];
 #pragma unroll
-          for (int f = 0; f < 8; f++) B.uout[f * nc + cc] = res[f];
+          for (int f = 0; f < 8; f++) store_value<MIX>(B, f * nc + cc, res[f], is_base);
           double gg[5];
           if (a2 == 0 && b == 0 && cz == 0) {
 #pragma unroll
@@ -599,25 +611,31 @@ __global__ void __launch_bounds__(s3::NT, 3) stage3d_fast(const KParams P, const
   }
 }
 
-template <int MODE>
+template <int MODE, bool MIX>
 static cudaError_t launch_stage3d(const KParams& K, const KBufs& B, cudaStream_t st) {
   dim3 grid((K.n0 - 4 + s3::T0 - 1) / s3::T0, (K.n1 - 4 + s3::T1 - 1) / s3::T1,
             (K.n2 - 4 + s3::T2 - 1) / s3::T2);
   if (K.has_bg)
-    stage3d_fast<MODE, true><<<grid, s3::NT, s3::smem_bytes(), st>>>(K, B);
+    stage3d_fast<MODE, true, MIX><<<grid, s3::NT, s3::smem_bytes<MIX>(), st>>>(K, B);
   else
-    stage3d_fast<MODE, false><<<grid, s3::NT, s3::smem_bytes(), st>>>(K, B);
+    stage3d_fast<MODE, false, MIX><<<grid, s3::NT, s3::smem_bytes<MIX>(), st>>>(K, B);
   return cudaGetLastError();
 }
 
-static cudaError_t stage3d_set_attributes() {
+template <int MODE, bool BG, bool MIX>
+static cudaError_t stage3d_attr() {
+  return cudaFuncSetAttribute(stage3d_fast<MODE, BG, MIX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)s3::smem_bytes<MIX>());
+}
+
+cudaError_t stage3d_set_attributes() {
   cudaError_t e;
-  const int sb = (int)s3::smem_bytes();
-  if ((e = cudaFuncSetAttribute(stage3d_fast<SMAUG_INT_EULER, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb)))
-    return e;
-  if ((e = cudaFuncSetAttribute(stage3d_fast<SMAUG_INT_EULER, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb)))
-    return e;
-  if ((e = cudaFuncSetAttribute(stage3d_fast<SMAUG_INT_RK4, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb)))
-    return e;
-  return cudaFuncSetAttribute(stage3d_fast<SMAUG_INT_RK4, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
+  if ((e = stage3d_attr<SMAUG_INT_EULER, true, false>())) return e;
+  if ((e = stage3d_attr<SMAUG_INT_EULER, false, false>())) return e;
+  if ((e = stage3d_attr<SMAUG_INT_RK4, true, false>())) return e;
+  if ((e = stage3d_attr<SMAUG_INT_RK4, false, false>())) return e;
+  if ((e = stage3d_attr<SMAUG_INT_EULER, true, true>())) return e;
+  if ((e = stage3d_attr<SMAUG_INT_EULER, false, true>())) return e;
+  if ((e = stage3d_attr<SMAUG_INT_RK4, true, true>())) return e;
+  return stage3d_attr<SMAUG_INT_RK4, false, true>();
 }

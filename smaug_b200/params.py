@@ -21,6 +21,7 @@ INT_EULER = 0
 INT_RK4 = 1
 
 PREC_FP64 = 0
+PREC_MIXED = 1
 
 PAD_STRAY = 0
 PAD_ZERO = 1
@@ -109,7 +110,7 @@ def make_params(ndim=2, n=(132, 132, 1), dx=None, gamma=5.0 / 3.0, courant=0.3,
                 dtmax=1.0, dt=1.0e-8, moddton=1, hyperdifmom=1, chyp=0.2,
                 boundtype=None, integrator=INT_EULER, g=(0.0, 0.0, 0.0),
                 eta=0.0, xmin=(0.0, 0.0, 0.0), pad_model=PAD_STRAY,
-                driver=DRIVER_NONE, drv_amp=0.0, drv_period=0.0,
+                driver=DRIVER_NONE, drv_amp=0.0, drv_period=0.0, precision=PREC_FP64,
                 drv_x0=(0.0, 0.0, 0.0), drv_sigma=(0.0, 0.0, 0.0)):
     """Build a parameter block.  Defaults: the reference's Orszag-Tang model
     (models/iosmaugparams.h.ot) with a 0.3 Courant number; `chyp` may be a
@@ -138,7 +139,7 @@ def make_params(ndim=2, n=(132, 132, 1), dx=None, gamma=5.0 / 3.0, courant=0.3,
     p.moddton = moddton
     p.hyperdifmom = hyperdifmom
     p.integrator = integrator
-    p.precision = PREC_FP64
+    p.precision = precision
     p.pad_model = pad_model
     if isinstance(chyp, (int, float)):
         for f in range(MAXVAR):
