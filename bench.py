@@ -23,6 +23,11 @@ periodic x and y, hydrostatic background on 2 x 2 x 6 Mm with a uniform
 10 G vertical field, Gaussian vertical-velocity driver (200 m/s, 30 s period,
 sigma 0.2 Mm, centred at z = 0.1 Mm, x = y = 1 Mm), gravity 274 m/s^2.
 
+--workload ensemble: 64 uneven 2D runs (sizes drawn by seed from 64^2..512^2,
+Orszag-Tang and stratified driven slabs) advanced by one batch (one launch per
+stage for all runs, CUDA-graph cycles, autotuned launch shape), against the
+same runs stepped one by one; mixed precision unless --precision fp64.
+
 --impl reference: the reference has no CPU solver (every routine is a CUDA
 kernel), so the CPU baseline is the oracle, the FP64 restatement of the
 reference's kernels (oracle/), run with all host threads on a bounded
@@ -155,6 +160,104 @@ def workload(args, seed=1):
                               "hyperdiffusion, CFL 0.3, FP64, classical RK4" % (N, N))
 
 
+ENSEMBLE_SIZES = (64, 128, 192, 256, 384, 512)
+
+
+def make_ensemble(nruns=64, seed=5, precision=1):
+    """Uneven 2D runs: sizes drawn by seed from ENSEMBLE_SIZES, alternately
+    Orszag-Tang (seeded rho noise) and stratified driven slabs (2 x 6 Mm,
+    vertical dim 0, driver periods uniform in [10, 300] s), RK4."""
+    import numpy as np
+    from smaug_b200 import ic, params as P
+    rng = np.random.default_rng(seed)
+    runs = []
+    for r in range(nruns):
+        n = int(rng.choice(ENSEMBLE_SIZES))
+        if r % 2 == 0:
+            w, pos, dx = ic.orszag_tang(n, noise=1e-3, seed=seed + r)
+            p = P.make_params(ndim=2, n=(n + 4, n + 4, 1), dx=dx, courant=0.3, dtmax=1.0,
+                              integrator=P.INT_RK4, precision=precision)
+        else:
+            period = float(rng.uniform(10.0, 300.0))
+            w, pos, dx = ic.stratified(nz=n, nx=n, seed=seed + r, vz_sigma=10.0)
+            p = P.make_params(ndim=2, n=(n + 4, n + 4, 1), dx=dx, courant=0.3, dtmax=1.0,
+                              integrator=P.INT_RK4, precision=precision, g=(-274.0, 0.0),
+                              boundtype=(P.BC_CONTCD4, P.BC_PERIODIC), driver=P.DRIVER_GAUSS,
+                              drv_amp=200.0, drv_period=period, drv_x0=(0.1e6, 1.0e6),
+                              drv_sigma=(0.2e6, 0.2e6))
+        runs.append((p, w, pos, n * n))
+    return runs
+
+
+def ensemble_main(args):
+    """--workload ensemble: 64 uneven runs in one batch (one launch per stage
+    for all runs, 6-step CUDA graph cycles, autotuned launch shape) against
+    the same runs stepped one by one through their own engines."""
+    import torch
+    from smaug_b200 import engine
+    prec = 0 if args.precision == "fp64" else 1
+    runs = make_ensemble(args.nruns, precision=prec)
+    cells = sum(r[3] for r in runs)
+    warm = max(args.warmup, 4)
+    b = engine.Batch([r[0] for r in runs], [r[1] for r in runs], [r[2] for r in runs])
+    stream = torch.cuda.Stream()
+    b.set_stream(stream.cuda_stream)
+    b.step(warm)            # the first 4 steps time the launch-shape candidates
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(0) as clk:
+        ev0.record(stream)
+        b.step_async(args.steps)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    b.sync()
+    ms = ev0.elapsed_time(ev1)
+    shape = b.launch_shape()
+    b.close()
+    # one by one: each run alone, its own engine and stream, same step counts
+    ms_single = 0.0
+    for p, w, pos, nc in runs:
+        e = engine.Engine(p, w, pos)
+        e.set_stream(stream.cuda_stream)
+        e.step(warm)
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        e.step_async(args.steps)
+        ev1.record(stream)
+        e.sync()
+        torch.cuda.synchronize()
+        ms_single += ev0.elapsed_time(ev1)
+        e.close()
+    value = cells * args.steps / (ms / 1e3) / 1e6
+    single = cells * args.steps / (ms_single / 1e3) / 1e6
+    peak, pk_kind = peaks()
+    mbytes = alg_bytes_mixed(2) if prec else alg_bytes_per_cell_step(2)
+    achieved = mbytes * cells * args.steps / (ms / 1e3) / 1e9
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+        "warmup": warm, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 storage + hyperdiffusion, f64 rest" if prec else "f64",
+        "data": "synthetic",
+        "config": {"workload": "ensemble of %d uneven 2D runs (sizes from %s by seed, "
+                               "Orszag-Tang and stratified driven slabs), classical RK4"
+                               % (len(runs), list(ENSEMBLE_SIZES)),
+                   "interior_cells": cells, "sizes": [int(round(r[3] ** 0.5)) for r in runs],
+                   "precision": args.precision,
+                   "timing": "CUDA events on the launch stream, batch and each single run"},
+        "one_by_one": {"value": single, "unit": UNIT, "ms_per_step": ms_single / args.steps},
+        "speedup_vs_one_by_one": value / single,
+        "launch_shape": shape,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "alg_bytes_per_cell_step": mbytes,
+                     "peak_kind": pk_kind},
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+
+
 def dist_setup(args):
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -247,8 +350,10 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="ot", choices=["ot", "tube"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--workload", default="ot", choices=["ot", "tube", "ensemble"])
+    ap.add_argument("--nruns", type=int, default=64)
+    ap.add_argument("--precision", default=None, choices=["fp64", "mixed"],
+                    help="default: fp64 (ot, tube; mixed reported beside it), mixed (ensemble)")
     ap.add_argument("--n", type=int, default=None)
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--ref-sample", type=int, default=512)
@@ -263,6 +368,11 @@ def main():
     if args.precision == "mixed":
         args.mixed = False
     ws, rank, local = dist_setup(args)
+    if args.precision is None:
+        args.precision = "mixed" if args.workload == "ensemble" else "fp64"
+    if args.workload == "ensemble" and args.impl != "reference":
+        ensemble_main(args)
+        return
     if args.impl == "reference":
         reference_arm(args, ws, rank)
         if ws > 1:

@@ -170,6 +170,34 @@ int smaug_write_out(smaug_handle_t h, const char* path, const char* name,
 /* Release all device memory of the handle. */
 int smaug_destroy(smaug_handle_t h);
 
+/* ---- batched ensemble of independent 2D runs ----------------------------
+ * No counterpart in the reference (one run per process there).  Runs of any
+ * size, boundary types, background fields and driver advance together with
+ * classical RK4: every stage of every run is one launch over the tile list of
+ * all runs, and a cycle of 6 steps is captured once into a CUDA graph and
+ * replayed.  All runs share one precision form.  The first 4 steps time 4
+ * launch shapes (1 and 2 blocks per SM, the occupancy limit per SM, one block
+ * per tile) and keep the fastest; results do not depend on the shape.  Each
+ * run's results equal those of the same run stepped alone with smaug_step. */
+typedef struct smaug_batch_s* smaug_batch_t;
+
+/* params[r], w[r], pos[r]: as smaug_create for run r (2D, integrator RK4) */
+int smaug_batch_create(int32_t nruns, const smaug_params_t* const* params, const double* const* w,
+                       const double* const* pos, smaug_batch_t* out);
+/* advance every run by nsteps RK4 steps; waits and reports non-finite values */
+int smaug_batch_step(smaug_batch_t b, int32_t nsteps);
+/* enqueue without waiting / wait and report; launch on a caller stream (NULL:
+   the batch's own) */
+int smaug_batch_step_async(smaug_batch_t b, int32_t nsteps);
+int smaug_batch_sync(smaug_batch_t b);
+int smaug_batch_set_stream(smaug_batch_t b, void* stream);
+/* state / time of run `run`, as smaug_get_state / smaug_get_time */
+int smaug_batch_get_state(smaug_batch_t b, int32_t run, double* w);
+int smaug_batch_get_time(smaug_batch_t b, int32_t run, int64_t* it, double* t, double* dt);
+/* chosen grid (0 before tuning), the 4 candidate grids and their step times in ms */
+int smaug_batch_launch_shape(smaug_batch_t b, int32_t* grid, int32_t* candidates, float* ms);
+int smaug_batch_destroy(smaug_batch_t b);
+
 /* Message of the calling thread's last failure ("" if none). */
 const char* smaug_last_error(void);
 

@@ -15,7 +15,8 @@ ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libsmaug_b200.so")
 OBJDIR = os.path.join(HERE, "_build")
 CSRC = os.path.join(HERE, "csrc")
-SRCS = [os.path.join(CSRC, f) for f in ("engine.cu", "stage2d.cu", "stage3d.cu", "host_io.cpp")]
+SRCS = [os.path.join(CSRC, f) for f in ("engine.cu", "stage2d.cu", "stage3d.cu", "batch.cu",
+                                         "host_io.cpp")]
 HEADERS = [os.path.join(CSRC, f) for f in sorted(os.listdir(CSRC)) if f.endswith((".h", ".cuh"))] + [
     os.path.join(ROOT, "include", "smaug_b200.h")]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

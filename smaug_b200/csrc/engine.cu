@@ -435,11 +435,12 @@ static int reset_derived(Engine* e) {
   return SMAUG_OK;
 }
 
-// one stage launch; uin/un/uout are the FP64 buffers or the float buffers
-// of the mixed form (un_lo / uout_lo: low parts where a base state is read
-// or written)
-static int launch_stage(Engine* e, int mode, int stage, const void* uin, const void* un,
-                        const float* un_lo, void* uout, float* uout_lo) {
+// kernel buffer block of one stage launch; uin/un/uout are the FP64 buffers
+// or the float buffers of the mixed form (un_lo / uout_lo: low parts where a
+// base state is read or written); `ring` = the launch's CFL-maxima ring slot
+// (stage_count mod 3), `parity` = the step's dt/t double-buffer index
+static KBufs fill_kbufs(const Engine* e, int mode, int stage, int parity, int ring, const void* uin,
+                        const void* un, const float* un_lo, void* uout, float* uout_lo) {
   KBufs B{};
   B.uin = uin;
   B.un = un;
@@ -453,23 +454,53 @@ static int launch_stage(Engine* e, int mode, int stage, const void* uin, const v
     B.pos[d] = e->d_pos[d];
     B.padsrc[d] = e->d_pad[d];
   }
-  long s = e->stage_count;
-  B.cmax_in = reinterpret_cast<const double*>(e->d_cmax + 3 * (s % 3));
-  B.cmax_out = e->d_cmax + 3 * ((s + 1) % 3);
-  B.cmax_clear = e->d_cmax + 3 * ((s + 2) % 3);
-  B.dt_prev = e->d_dt + e->parity;
-  B.dt_new = e->d_dt + (1 - e->parity);
-  B.t_prev = e->d_t + e->parity;
-  B.t_new = e->d_t + (1 - e->parity);
+  B.cmax_in = reinterpret_cast<const double*>(e->d_cmax + 3 * ring);
+  B.cmax_out = e->d_cmax + 3 * ((ring + 1) % 3);
+  B.cmax_clear = e->d_cmax + 3 * ((ring + 2) % 3);
+  B.dt_prev = e->d_dt + parity;
+  B.dt_new = e->d_dt + (1 - parity);
+  B.t_prev = e->d_t + parity;
+  B.t_new = e->d_t + (1 - parity);
   B.flags = e->d_flags;
   B.mode = mode;
   B.stage = stage;
+  return B;
+}
+
+static int launch_stage(Engine* e, int mode, int stage, const void* uin, const void* un,
+                        const float* un_lo, void* uout, float* uout_lo) {
+  KBufs B = fill_kbufs(e, mode, stage, e->parity, (int)(e->stage_count % 3), uin, un, un_lo, uout,
+                       uout_lo);
   if (e->nd == 3)
     CUDA_TRY(launch_stage3d_any(mode, e->mix, e->K, B, e->stream));
   else
     CUDA_TRY(launch_stage2d_any(mode, e->mix, e->K, B, e->stream));
   e->stage_count++;
   return SMAUG_OK;
+}
+
+// RK4 stage buffers of an engine: (uin, un, un_lo, uout, uout_lo) of stage s;
+// the base state stays in place for RK4 (FP64: d_u[cur]; mixed: h0/h1)
+static KBufs rk4_kbufs(const Engine* e, int stage, int parity, int ring) {
+  if (e->mix) {
+    float* hi = e->d_h[0];
+    float* lo = e->d_h[1];
+    switch (stage) {
+      case 0: return fill_kbufs(e, SMAUG_INT_RK4, 0, parity, ring, hi, hi, lo, e->d_h[2], nullptr);
+      case 1: return fill_kbufs(e, SMAUG_INT_RK4, 1, parity, ring, e->d_h[2], hi, lo, e->d_h[3], nullptr);
+      case 2: return fill_kbufs(e, SMAUG_INT_RK4, 2, parity, ring, e->d_h[3], hi, lo, e->d_h[2], nullptr);
+      default: return fill_kbufs(e, SMAUG_INT_RK4, 3, parity, ring, e->d_h[2], hi, lo, hi, lo);
+    }
+  }
+  double* un = e->d_u[e->cur];
+  double* a = e->d_u[(e->cur + 1) % 3];
+  double* b = e->d_u[(e->cur + 2) % 3];
+  switch (stage) {
+    case 0: return fill_kbufs(e, SMAUG_INT_RK4, 0, parity, ring, un, un, nullptr, a, nullptr);
+    case 1: return fill_kbufs(e, SMAUG_INT_RK4, 1, parity, ring, a, un, nullptr, b, nullptr);
+    case 2: return fill_kbufs(e, SMAUG_INT_RK4, 2, parity, ring, b, un, nullptr, a, nullptr);
+    default: return fill_kbufs(e, SMAUG_INT_RK4, 3, parity, ring, a, un, nullptr, un, nullptr);
+  }
 }
 
 static int sync_check(Engine* e) {
@@ -684,6 +715,301 @@ extern "C" int smaug_destroy(smaug_handle_t h) {
   Engine* e = H(h);
   cudaStreamSynchronize(e->stream);
   smaug::free_engine(e);
+  return SMAUG_OK;
+}
+
+// ===========================================================================
+// Batched ensemble of 2D runs
+// ===========================================================================
+// Independent runs advance together: each stage of every run is one launch of
+// stage2d_batch over the concatenated tile list of all runs, and a cycle of 6
+// RK4 steps (the period of the dt/t double buffers, 2, and of the CFL-maxima
+// ring, 3 slots advanced 4 times per step) is captured once into a CUDA graph
+// and replayed.  Each run keeps its own engine state (buffers, dt, time, CFL
+// maxima), so a run's results are those of the same run stepped alone.
+namespace smaug {
+
+constexpr int BATCH_CYCLE = 6;
+
+struct Batch {
+  std::vector<Engine*> runs;
+  bool mix = false;
+  cudaStream_t stream = nullptr;
+  KParams* d_K = nullptr;   // [nruns]
+  KBufs* d_B = nullptr;     // [4 stages][2 parities][3 ring slots][nruns]
+  int4* d_tiles = nullptr;  // (run, tile x, tile y)
+  int ntiles = 0;
+  int grid = 0;             // persistent blocks per launch (0: not chosen yet)
+  int grid_candidates[4] = {0, 0, 0, 0};
+  float grid_ms[4] = {0, 0, 0, 0};
+  int tuned = 0;            // candidates timed so far
+  long steps = 0;
+  cudaGraphExec_t cycle = nullptr;
+  cudaStream_t own_stream = nullptr;  // the batch's stream while a caller stream is set
+};
+
+static void free_batch(Batch* b) {
+  if (!b) return;
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  if (b->cycle) cudaGraphExecDestroy(b->cycle);
+  cudaFree(b->d_K);
+  cudaFree(b->d_B);
+  cudaFree(b->d_tiles);
+  for (Engine* e : b->runs) free_engine(e);
+  cudaStreamDestroy(b->own_stream ? b->own_stream : b->stream);
+  delete b;
+}
+
+static int batch_variant(int stage, int parity, int ring) { return (stage * 2 + parity) * 3 + ring; }
+
+// one RK4 step of every run, starting at global step index k of the batch
+static int batch_enqueue_step(Batch* b, long k, int grid) {
+  const int nr = (int)b->runs.size();
+  const int parity = (int)(k % 2);
+  for (int s = 0; s < 4; s++) {
+    const int ring = (int)((4 * k + s) % 3);
+    CUDA_TRY(launch_batch2d(SMAUG_INT_RK4, b->mix, b->d_K, b->d_B + (size_t)batch_variant(s, parity, ring) * nr,
+                            b->d_tiles, b->ntiles, grid, b->stream));
+  }
+  return SMAUG_OK;
+}
+
+static void batch_advance_bookkeeping(Batch* b, long nsteps) {
+  for (Engine* e : b->runs) {
+    e->stage_count += 4 * nsteps;
+    if (nsteps % 2) e->parity = 1 - e->parity;
+    e->it += nsteps;
+  }
+  b->steps += nsteps;
+}
+
+static int batch_create(int nruns, const smaug_params_t* const* params, const double* const* w,
+                        const double* const* pos, Batch** out) {
+  if (nruns < 1 || !params || !w || !pos || !out) return set_error(SMAUG_E_INVALID, "bad batch arguments");
+  Batch* b = new Batch();
+  auto fail = [&](int code) { free_batch(b); return code; };
+  for (int r = 0; r < nruns; r++) {
+    if (!params[r]) return fail(set_error(SMAUG_E_INVALID, "run %d: null parameter block", r));
+    if (params[r]->ndim != 2) return fail(set_error(SMAUG_E_UNSUPPORTED, "run %d: batches are 2D only", r));
+    if (params[r]->integrator != SMAUG_INT_RK4)
+      return fail(set_error(SMAUG_E_UNSUPPORTED, "run %d: batches step with RK4", r));
+    if (params[r]->precision != params[0]->precision)
+      return fail(set_error(SMAUG_E_UNSUPPORTED, "run %d: all runs of a batch share one precision form", r));
+    Engine* e = nullptr;
+    int rc = create(params[r], w[r], pos[r], &e);
+    if (rc) return fail(rc);
+    b->runs.push_back(e);
+    rc = reset_derived(e);
+    if (rc) return fail(rc);
+  }
+  b->mix = (params[0]->precision == SMAUG_PREC_MIXED);
+  cudaError_t ce = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+  if (ce != cudaSuccess) return fail(set_error(SMAUG_E_CUDA, "stream: %s", cudaGetErrorString(ce)));
+  for (Engine* e : b->runs) {
+    ce = cudaStreamSynchronize(e->stream);
+    if (ce != cudaSuccess) return fail(set_error(SMAUG_E_CUDA, "create: %s", cudaGetErrorString(ce)));
+    e->stream = b->stream;
+  }
+  // parameter blocks, the 24 buffer-block variants of every run, the tile list
+  std::vector<KParams> K(nruns);
+  std::vector<KBufs> B((size_t)24 * nruns);
+  std::vector<int4> tiles;
+  for (int r = 0; r < nruns; r++) {
+    Engine* e = b->runs[r];
+    K[r] = e->K;
+    K[r].has_bg = 1;
+    for (int s = 0; s < 4; s++)
+      for (int par = 0; par < 2; par++)
+        for (int ring = 0; ring < 3; ring++)
+          B[(size_t)batch_variant(s, par, ring) * nruns + r] = rk4_kbufs(e, s, par, ring);
+    const int tx = (e->K.n0 - 4 + TX - 1) / TX, ty = (e->K.n1 - 4 + TY - 1) / TY;
+    for (int j = 0; j < ty; j++)
+      for (int i = 0; i < tx; i++) tiles.push_back(make_int4(r, i, j, 0));
+  }
+  b->ntiles = (int)tiles.size();
+#define B_TRY(call)                                                                             \
+  do {                                                                                          \
+    cudaError_t _e = (call);                                                                    \
+    if (_e != cudaSuccess)                                                                      \
+      return fail(set_error(_e == cudaErrorMemoryAllocation ? SMAUG_E_NOMEM : SMAUG_E_CUDA,    \
+                            "%s: %s", #call, cudaGetErrorString(_e)));                         \
+  } while (0)
+  B_TRY(cudaMalloc(&b->d_K, sizeof(KParams) * nruns));
+  B_TRY(cudaMalloc(&b->d_B, sizeof(KBufs) * B.size()));
+  B_TRY(cudaMalloc(&b->d_tiles, sizeof(int4) * tiles.size()));
+  B_TRY(cudaMemcpy(b->d_K, K.data(), sizeof(KParams) * nruns, cudaMemcpyHostToDevice));
+  B_TRY(cudaMemcpy(b->d_B, B.data(), sizeof(KBufs) * B.size(), cudaMemcpyHostToDevice));
+  B_TRY(cudaMemcpy(b->d_tiles, tiles.data(), sizeof(int4) * tiles.size(), cudaMemcpyHostToDevice));
+  B_TRY(batch2d_set_attributes());
+  // launch-shape candidates: 1, 2 or the occupancy limit of blocks per SM
+  // (persistent), or one block per tile
+  int dev = 0, nsm = 0;
+  B_TRY(cudaGetDevice(&dev));
+  B_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  int occ = batch2d_max_blocks_per_sm(b->mix);
+  if (occ < 1) occ = 1;
+  b->grid_candidates[0] = nsm;
+  b->grid_candidates[1] = 2 * nsm < b->ntiles ? 2 * nsm : b->ntiles;
+  b->grid_candidates[2] = occ * nsm < b->ntiles ? occ * nsm : b->ntiles;
+  b->grid_candidates[3] = b->ntiles;
+#undef B_TRY
+  *out = b;
+  return SMAUG_OK;
+}
+
+// Launch-shape autotuning: the first four steps run with the four candidate
+// grids, each timed with events; the fastest is kept.  The grid only changes
+// which block processes which tile, so results do not depend on it.
+static int batch_tune(Batch* b, int* nsteps) {
+  cudaEvent_t ev[2];
+  CUDA_TRY(cudaEventCreate(&ev[0]));
+  CUDA_TRY(cudaEventCreate(&ev[1]));
+  for (int c = b->tuned; c < 4 && *nsteps > 0; c++) {
+    CUDA_TRY(cudaEventRecord(ev[0], b->stream));
+    int rc = batch_enqueue_step(b, b->steps, b->grid_candidates[c]);
+    if (rc) return rc;
+    CUDA_TRY(cudaEventRecord(ev[1], b->stream));
+    CUDA_TRY(cudaEventSynchronize(ev[1]));
+    CUDA_TRY(cudaEventElapsedTime(&b->grid_ms[c], ev[0], ev[1]));
+    batch_advance_bookkeeping(b, 1);
+    (*nsteps)--;
+    b->tuned = c + 1;
+  }
+  if (b->tuned == 4) {
+    int best = 0;
+    for (int c = 1; c < 4; c++)
+      if (b->grid_ms[c] < b->grid_ms[best]) best = c;
+    b->grid = b->grid_candidates[best];
+  }
+  cudaEventDestroy(ev[0]);
+  cudaEventDestroy(ev[1]);
+  return SMAUG_OK;
+}
+
+static int batch_enqueue(Batch* b, int nsteps) {
+  if (!b->grid) {
+    int rc = batch_tune(b, &nsteps);
+    if (rc) return rc;
+  }
+  while (nsteps > 0) {
+    if (b->steps % BATCH_CYCLE == 0 && nsteps >= BATCH_CYCLE) {
+      if (!b->cycle) {
+        cudaGraph_t g = nullptr;
+        CUDA_TRY(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+        int rc = SMAUG_OK;
+        for (int k = 0; k < BATCH_CYCLE && !rc; k++) rc = batch_enqueue_step(b, k, b->grid);
+        cudaError_t ce = cudaStreamEndCapture(b->stream, &g);
+        if (rc) return rc;
+        if (ce != cudaSuccess) return set_error(SMAUG_E_CUDA, "graph capture: %s", cudaGetErrorString(ce));
+        ce = cudaGraphInstantiate(&b->cycle, g, 0);
+        cudaGraphDestroy(g);
+        if (ce != cudaSuccess) return set_error(SMAUG_E_CUDA, "graph instantiate: %s", cudaGetErrorString(ce));
+      }
+      CUDA_TRY(cudaGraphLaunch(b->cycle, b->stream));
+      batch_advance_bookkeeping(b, BATCH_CYCLE);
+      nsteps -= BATCH_CYCLE;
+    } else {
+      int rc = batch_enqueue_step(b, b->steps, b->grid);
+      if (rc) return rc;
+      batch_advance_bookkeeping(b, 1);
+      nsteps--;
+    }
+  }
+  return SMAUG_OK;
+}
+
+static int batch_sync(Batch* b) {
+  CUDA_TRY(cudaStreamSynchronize(b->stream));
+  for (Engine* e : b->runs) {
+    int rc = sync_check(e);
+    if (rc) return rc;
+  }
+  return SMAUG_OK;
+}
+
+}  // namespace smaug
+
+using smaug::Batch;
+static Batch* HB(smaug_batch_t h) { return reinterpret_cast<Batch*>(h); }
+
+extern "C" int smaug_batch_create(int32_t nruns, const smaug_params_t* const* params,
+                                  const double* const* w, const double* const* pos,
+                                  smaug_batch_t* out) {
+  smaug::clear_error();
+  if (!out) return smaug::set_error(SMAUG_E_INVALID, "null handle pointer");
+  *out = nullptr;
+  Batch* b = nullptr;
+  int rc = smaug::batch_create(nruns, params, w, pos, &b);
+  if (rc) return rc;
+  *out = reinterpret_cast<smaug_batch_t>(b);
+  return SMAUG_OK;
+}
+
+extern "C" int smaug_batch_step(smaug_batch_t h, int32_t nsteps) {
+  smaug::clear_error();
+  if (!h) return smaug::set_error(SMAUG_E_INVALID, "null handle");
+  if (nsteps < 0) return smaug::set_error(SMAUG_E_INVALID, "nsteps < 0");
+  int rc = smaug::batch_enqueue(HB(h), nsteps);
+  if (rc) return rc;
+  return smaug::batch_sync(HB(h));
+}
+
+extern "C" int smaug_batch_step_async(smaug_batch_t h, int32_t nsteps) {
+  smaug::clear_error();
+  if (!h) return smaug::set_error(SMAUG_E_INVALID, "null handle");
+  if (nsteps < 0) return smaug::set_error(SMAUG_E_INVALID, "nsteps < 0");
+  return smaug::batch_enqueue(HB(h), nsteps);
+}
+
+extern "C" int smaug_batch_sync(smaug_batch_t h) {
+  smaug::clear_error();
+  if (!h) return smaug::set_error(SMAUG_E_INVALID, "null handle");
+  return smaug::batch_sync(HB(h));
+}
+
+extern "C" int smaug_batch_set_stream(smaug_batch_t h, void* stream) {
+  smaug::clear_error();
+  if (!h) return smaug::set_error(SMAUG_E_INVALID, "null handle");
+  Batch* b = HB(h);
+  CUDA_TRY(cudaStreamSynchronize(b->stream));
+  if (!b->own_stream) b->own_stream = b->stream;
+  b->stream = stream ? static_cast<cudaStream_t>(stream) : b->own_stream;
+  for (smaug::Engine* e : b->runs) e->stream = b->stream;
+  return SMAUG_OK;
+}
+
+extern "C" int smaug_batch_get_state(smaug_batch_t h, int32_t run, double* w) {
+  smaug::clear_error();
+  if (!h) return smaug::set_error(SMAUG_E_INVALID, "null handle");
+  Batch* b = HB(h);
+  if (run < 0 || run >= (int)b->runs.size()) return smaug::set_error(SMAUG_E_INVALID, "run %d out of range", run);
+  return smaug_get_state(reinterpret_cast<smaug_handle_t>(b->runs[run]), w);
+}
+
+extern "C" int smaug_batch_get_time(smaug_batch_t h, int32_t run, int64_t* it, double* t, double* dt) {
+  smaug::clear_error();
+  if (!h) return smaug::set_error(SMAUG_E_INVALID, "null handle");
+  Batch* b = HB(h);
+  if (run < 0 || run >= (int)b->runs.size()) return smaug::set_error(SMAUG_E_INVALID, "run %d out of range", run);
+  return smaug_get_time(reinterpret_cast<smaug_handle_t>(b->runs[run]), it, t, dt);
+}
+
+extern "C" int smaug_batch_launch_shape(smaug_batch_t h, int32_t* grid, int32_t* candidates, float* ms) {
+  smaug::clear_error();
+  if (!h) return smaug::set_error(SMAUG_E_INVALID, "null handle");
+  Batch* b = HB(h);
+  if (grid) *grid = b->grid;
+  for (int c = 0; c < 4; c++) {
+    if (candidates) candidates[c] = b->grid_candidates[c];
+    if (ms) ms[c] = b->grid_ms[c];
+  }
+  return SMAUG_OK;
+}
+
+extern "C" int smaug_batch_destroy(smaug_batch_t h) {
+  smaug::clear_error();
+  if (!h) return SMAUG_OK;
+  smaug::free_batch(HB(h));
   return SMAUG_OK;
 }
 

@@ -220,4 +220,11 @@ cudaError_t launch_stage3d_any(int mode, bool mix, const KParams& K, const KBufs
 cudaError_t stage2d_set_attributes();
 cudaError_t stage3d_set_attributes();
 
+// batched 2D stages (batch.cu): Ks/Bs per run in device memory, tiles =
+// (run, tile x, tile y) work list, `grid` persistent blocks
+cudaError_t launch_batch2d(int mode, bool mix, const KParams* Ks, const KBufs* Bs, const int4* tiles,
+                           int ntiles, int grid, cudaStream_t st);
+cudaError_t batch2d_set_attributes();
+int batch2d_max_blocks_per_sm(bool mix);
+
 }  // namespace smaug

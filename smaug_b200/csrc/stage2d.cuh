@@ -309,8 +309,10 @@ __device__ __forceinline__ void hyper_pass(const T2<BG, MIX>& T, const KParams& 
   __syncthreads();
 }
 
+// The stage for tile (bx, by) of one grid; the single-run kernel below and
+// the batched kernel (batch.cu) call it.
 template <int MODE, bool BG, bool MIX>
-__global__ void __launch_bounds__(NTHREADS, 3) stage2d_fast(const KParams P, const KBufs B) {
+__device__ __forceinline__ void stage2d_body(const KParams& P, const KBufs& B, int bx, int by) {
   using ST = typename Form<MIX>::S;
   extern __shared__ double smem[];
   T2<BG, MIX> T;
@@ -327,8 +329,8 @@ __global__ void __launch_bounds__(NTHREADS, 3) stage2d_fast(const KParams P, con
   T.rd1 = T.rd0 + RX;
   T.U = T.rd1 + RY;
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
-  T.x0 = 2 + blockIdx.x * TX;
-  T.y0 = 2 + blockIdx.y * TY;
+  T.x0 = 2 + bx * TX;
+  T.y0 = 2 + by * TY;
   const int n0 = P.n0, n1 = P.n1;
   const long nc = P.ncell;
   const ST* uin = static_cast<const ST*>(B.uin);
@@ -382,7 +384,7 @@ __global__ void __launch_bounds__(NTHREADS, 3) stage2d_fast(const KParams P, con
   double dt, tstage;
   if (B.stage == 0) {
     dt = device_dt(P, B.cmax_in, *B.dt_prev, 2);
-    if (blockIdx.x == 0 && blockIdx.y == 0 && tid == 0) {
+    if (bx == 0 && by == 0 && tid == 0) {
       *B.dt_new = dt;
       *B.t_new = *B.t_prev + dt;
       B.cmax_clear[0] = B.cmax_clear[1] = B.cmax_clear[2] = 0ull;
@@ -391,7 +393,7 @@ __global__ void __launch_bounds__(NTHREADS, 3) stage2d_fast(const KParams P, con
   } else {
     dt = *B.dt_new;
     tstage = *B.t_prev + (B.stage == 3 ? dt : 0.5 * dt);
-    if (blockIdx.x == 0 && blockIdx.y == 0 && tid == 0)
+    if (bx == 0 && by == 0 && tid == 0)
       B.cmax_clear[0] = B.cmax_clear[1] = B.cmax_clear[2] = 0ull;
   }
   __syncthreads();
@@ -571,6 +573,11 @@ __global__ void __launch_bounds__(NTHREADS, 3) stage2d_fast(const KParams P, con
   }
 }
 
+template <int MODE, bool BG, bool MIX>
+__global__ void __launch_bounds__(NTHREADS, 3) stage2d_fast(const KParams P, const KBufs B) {
+  stage2d_body<MODE, BG, MIX>(P, B, blockIdx.x, blockIdx.y);
+}
+
 // launch helper: picks the background specialisation
 template <int MODE, bool MIX>
 static cudaError_t launch_stage2d(const KParams& K, const KBufs& B, cudaStream_t st) {
@@ -588,16 +595,4 @@ template <int MODE, bool BG, bool MIX>
 static cudaError_t stage2d_attr() {
   return cudaFuncSetAttribute(stage2d_fast<MODE, BG, MIX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)s2::smem_bytes<BG, MIX>());
-}
-
-cudaError_t stage2d_set_attributes() {
-  cudaError_t e;
-  if ((e = stage2d_attr<SMAUG_INT_EULER, true, false>())) return e;
-  if ((e = stage2d_attr<SMAUG_INT_EULER, false, false>())) return e;
-  if ((e = stage2d_attr<SMAUG_INT_RK4, true, false>())) return e;
-  if ((e = stage2d_attr<SMAUG_INT_RK4, false, false>())) return e;
-  if ((e = stage2d_attr<SMAUG_INT_EULER, true, true>())) return e;
-  if ((e = stage2d_attr<SMAUG_INT_EULER, false, true>())) return e;
-  if ((e = stage2d_attr<SMAUG_INT_RK4, true, true>())) return e;
-  return stage2d_attr<SMAUG_INT_RK4, false, true>();
 }

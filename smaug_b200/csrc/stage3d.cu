@@ -12,4 +12,16 @@ cudaError_t launch_stage3d_any(int mode, bool mix, const KParams& K, const KBufs
   return mix ? launch_stage3d<SMAUG_INT_RK4, true>(K, B, st) : launch_stage3d<SMAUG_INT_RK4, false>(K, B, st);
 }
 
+cudaError_t stage3d_set_attributes() {
+  cudaError_t e;
+  if ((e = stage3d_attr<SMAUG_INT_EULER, true, false>())) return e;
+  if ((e = stage3d_attr<SMAUG_INT_EULER, false, false>())) return e;
+  if ((e = stage3d_attr<SMAUG_INT_RK4, true, false>())) return e;
+  if ((e = stage3d_attr<SMAUG_INT_RK4, false, false>())) return e;
+  if ((e = stage3d_attr<SMAUG_INT_EULER, true, true>())) return e;
+  if ((e = stage3d_attr<SMAUG_INT_EULER, false, true>())) return e;
+  if ((e = stage3d_attr<SMAUG_INT_RK4, true, true>())) return e;
+  return stage3d_attr<SMAUG_INT_RK4, false, true>();
+}
+
 }  // namespace smaug

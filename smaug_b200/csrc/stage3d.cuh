@@ -627,15 +627,3 @@ static cudaError_t stage3d_attr() {
   return cudaFuncSetAttribute(stage3d_fast<MODE, BG, MIX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)s3::smem_bytes<MIX>());
 }
-
-cudaError_t stage3d_set_attributes() {
-  cudaError_t e;
-  if ((e = stage3d_attr<SMAUG_INT_EULER, true, false>())) return e;
-  if ((e = stage3d_attr<SMAUG_INT_EULER, false, false>())) return e;
-  if ((e = stage3d_attr<SMAUG_INT_RK4, true, false>())) return e;
-  if ((e = stage3d_attr<SMAUG_INT_RK4, false, false>())) return e;
-  if ((e = stage3d_attr<SMAUG_INT_EULER, true, true>())) return e;
-  if ((e = stage3d_attr<SMAUG_INT_EULER, false, true>())) return e;
-  if ((e = stage3d_attr<SMAUG_INT_RK4, true, true>())) return e;
-  return stage3d_attr<SMAUG_INT_RK4, false, true>();
-}

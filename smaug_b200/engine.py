@@ -20,7 +20,9 @@ EXPORTS = [
     "smaug_set_state", "smaug_get_time", "smaug_get_cmax", "smaug_write_out",
     "smaug_destroy", "smaug_last_error", "smaug_version", "smaug_read_ini",
     "smaug_write_out_host", "smaug_grid_metric", "smaug_step_async", "smaug_sync",
-    "smaug_set_stream", "smaug_euler_step_noalloc",
+    "smaug_set_stream", "smaug_euler_step_noalloc", "smaug_batch_create", "smaug_batch_step",
+    "smaug_batch_get_state", "smaug_batch_get_time", "smaug_batch_launch_shape",
+    "smaug_batch_destroy", "smaug_batch_step_async", "smaug_batch_sync", "smaug_batch_set_stream",
 ]
 
 ERRORS = {1: "invalid", 2: "cuda", 3: "nomem", 4: "io", 5: "format", 6: "unsupported",
@@ -68,6 +70,18 @@ def lib():
         L.smaug_write_out_host.argtypes = [ctypes.c_char_p, vp, dp, dp, ctypes.c_char_p,
                                            ctypes.c_int32, ctypes.c_double]
         L.smaug_grid_metric.argtypes = [ctypes.c_int32, ctypes.POINTER(ctypes.c_int32), dp, dp]
+        L.smaug_batch_create.argtypes = [ctypes.c_int32, ctypes.POINTER(vp), ctypes.POINTER(dp),
+                                         ctypes.POINTER(dp), ctypes.POINTER(vp)]
+        L.smaug_batch_step.argtypes = [vp, ctypes.c_int32]
+        L.smaug_batch_step_async.argtypes = [vp, ctypes.c_int32]
+        L.smaug_batch_sync.argtypes = [vp]
+        L.smaug_batch_set_stream.argtypes = [vp, vp]
+        L.smaug_batch_get_state.argtypes = [vp, ctypes.c_int32, dp]
+        L.smaug_batch_get_time.argtypes = [vp, ctypes.c_int32, ctypes.POINTER(ctypes.c_int64), dp, dp]
+        L.smaug_batch_launch_shape.argtypes = [vp, ctypes.POINTER(ctypes.c_int32),
+                                               ctypes.POINTER(ctypes.c_int32),
+                                               ctypes.POINTER(ctypes.c_float)]
+        L.smaug_batch_destroy.argtypes = [vp]
         _lib = L
     return _lib
 
@@ -187,6 +201,77 @@ class Engine:
 
     def __exit__(self, *a):
         self.close()
+
+
+class Batch:
+    """An ensemble of independent 2D runs advanced together (RK4): one launch
+    per stage for all runs, a 6-step cycle replayed from a CUDA graph."""
+
+    def __init__(self, params_list, w_list, pos_list):
+        n = len(params_list)
+        if not (n == len(w_list) == len(pos_list)) or n == 0:
+            raise ValueError("params, states and positions must be non-empty lists of one length")
+        self.params = list(params_list)
+        self.w = [np.ascontiguousarray(w, dtype=np.float64) for w in w_list]
+        self.pos = [np.ascontiguousarray(p, dtype=np.float64) for p in pos_list]
+        for p, w, x in zip(self.params, self.w, self.pos):
+            if w.shape != (p.nvar,) + p.shape or x.shape != (p.ndim,) + p.shape:
+                raise ValueError("state/positions shape does not match its parameter block")
+        vp = ctypes.c_void_p
+        dp = ctypes.POINTER(ctypes.c_double)
+        pa = (vp * n)(*[ctypes.cast(ctypes.byref(p), vp) for p in self.params])
+        wa = (dp * n)(*[_dp(w) for w in self.w])
+        xa = (dp * n)(*[_dp(x) for x in self.pos])
+        h = vp()
+        _check(lib().smaug_batch_create(n, pa, wa, xa, ctypes.byref(h)))
+        self.h = h
+        self.n = n
+
+    def step(self, nsteps=1):
+        _check(lib().smaug_batch_step(self.h, int(nsteps)))
+        return self
+
+    def step_async(self, nsteps=1):
+        _check(lib().smaug_batch_step_async(self.h, int(nsteps)))
+        return self
+
+    def sync(self):
+        _check(lib().smaug_batch_sync(self.h))
+
+    def set_stream(self, stream_handle):
+        _check(lib().smaug_batch_set_stream(self.h, ctypes.c_void_p(stream_handle or None)))
+
+    def state(self, run):
+        p = self.params[run]
+        w = np.zeros((p.nvar,) + p.shape)
+        _check(lib().smaug_batch_get_state(self.h, int(run), _dp(w)))
+        return w
+
+    def time(self, run):
+        it = ctypes.c_int64(0)
+        t = ctypes.c_double(0)
+        dt = ctypes.c_double(0)
+        _check(lib().smaug_batch_get_time(self.h, int(run), ctypes.byref(it), ctypes.byref(t),
+                                          ctypes.byref(dt)))
+        return int(it.value), float(t.value), float(dt.value)
+
+    def launch_shape(self):
+        g = ctypes.c_int32(0)
+        cand = (ctypes.c_int32 * 4)()
+        ms = (ctypes.c_float * 4)()
+        _check(lib().smaug_batch_launch_shape(self.h, ctypes.byref(g), cand, ms))
+        return {"grid": int(g.value), "candidates": list(cand), "ms": [float(v) for v in ms]}
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().smaug_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def euler_step_noalloc(params, w_in_ptr, w_out_ptr, delx1d, dt, stream=None):

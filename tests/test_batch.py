@@ -1,0 +1,79 @@
+"""Batched ensemble (smaug_batch_*): runs of different sizes, boundary types,
+backgrounds and drivers advanced together must reproduce each run stepped
+alone through smaug_step.  Tolerance: relative L2 per evolved field <= 1e-12
+(FP64) and <= 1e-6 (mixed form: the two launch paths may contract multiply-adds
+differently in the float hyperdiffusion)."""
+import numpy as np
+import pytest
+
+from smaug_b200 import ic, params as P
+from tests.util import ot_rect, params_for, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+def slab(nz, nx, period, seed):
+    """stratified driven slab (vertical = dim 0), as in the ensemble benchmark"""
+    w, pos, dx = ic.stratified(nz=nz, nx=nx, seed=seed, vz_sigma=10.0)
+    p = P.make_params(ndim=2, n=(nz + 4, nx + 4, 1), dx=dx, courant=0.3, dtmax=1.0,
+                      integrator=P.INT_RK4, g=(-274.0, 0.0),
+                      boundtype=(P.BC_CONTCD4, P.BC_PERIODIC), driver=P.DRIVER_GAUSS,
+                      drv_amp=200.0, drv_period=period, drv_x0=(0.1e6, 1.0e6),
+                      drv_sigma=(0.2e6, 0.2e6))
+    return p, w, pos
+
+
+def ensemble(precision):
+    runs = []
+    for (nx, ny, seed) in [(64, 64, 1), (96, 80, 2), (37, 29, 3), (128, 128, 4)]:
+        w, pos, dx = ot_rect(nx, ny, seed=seed)
+        runs.append((params_for(w, dx, integrator=P.INT_RK4, precision=precision), w, pos))
+    p, w, pos = slab(48, 64, 30.0, 5)
+    p.precision = precision
+    runs.append((p, w, pos))
+    return runs
+
+
+@pytest.mark.parametrize("precision,tol", [(P.PREC_FP64, 1e-12), (P.PREC_MIXED, 1e-6)])
+def test_batch_matches_single_runs(engine_lib, precision, tol):
+    runs = ensemble(precision)
+    b = engine_lib.Batch([r[0] for r in runs], [r[1] for r in runs], [r[2] for r in runs])
+    b.step(13)  # 4 tuning steps, one 6-step graph cycle, 3 single steps
+    shape = b.launch_shape()
+    assert shape["grid"] in shape["candidates"]
+    for i, (p, w, pos) in enumerate(runs):
+        e = engine_lib.Engine(p, w, pos)
+        e.step(13)
+        ref = e.state()
+        it, t, dt = e.time()
+        e.close()
+        got = b.state(i)
+        for f in range(6):
+            assert rel_l2(got[f], ref[f]) <= tol, (i, f, rel_l2(got[f], ref[f]))
+        assert np.array_equal(got[6:], ref[6:])
+        bit, bt, bdt = b.time(i)
+        assert bit == it == 13
+        assert abs(bt - t) <= 1e-12 * abs(t)
+    b.step(7)  # continues from a cycle boundary that is not 0 mod 6
+    for i, (p, w, pos) in enumerate(runs[:2]):
+        e = engine_lib.Engine(p, w, pos)
+        e.step(20)
+        ref = e.state()
+        e.close()
+        got = b.state(i)
+        for f in range(6):
+            assert rel_l2(got[f], ref[f]) <= tol
+    b.close()
+
+
+def test_batch_rejects(engine_lib):
+    w, pos, dx = ot_rect(32, 32, seed=1)
+    pe = params_for(w, dx, integrator=P.INT_EULER)
+    with pytest.raises(engine_lib.SmaugError) as e:
+        engine_lib.Batch([pe], [w], [pos])
+    assert e.value.code == 6
+    p64 = params_for(w, dx, integrator=P.INT_RK4)
+    pmx = params_for(w, dx, integrator=P.INT_RK4, precision=P.PREC_MIXED)
+    with pytest.raises(engine_lib.SmaugError) as e:
+        engine_lib.Batch([p64, pmx], [w, w], [pos, pos])
+    assert e.value.code == 6
