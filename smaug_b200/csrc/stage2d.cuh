@@ -23,20 +23,23 @@
 // scratch:
 //   flux phase:  5 flux arrays on the tile +-2 cells along the direction
 //                (+ 2 velocity arrays when background fields are present)
-//   hyperdiffusion phase: q on the tile +-3 along dim / +-1 across,
-//                nu_r, nu_l and two cross-term arrays on the tile +-1 across.
+//   hyperdiffusion phase: q of one field on the whole region (shared by the
+//                passes of both directions), the nu ratio on the tile
+//                extended by one cell along the direction, two cross-term
+//                arrays on the tile +-1 across.
 #pragma once
 
 // (included inside namespace smaug)
 namespace s2 {
 constexpr int FSZ = (TX + 4) * TY > TX * (TY + 4) ? (TX + 4) * TY : TX * (TY + 4);
-constexpr int QSZ = RX * (TY + 2) > (TX + 2) * RY ? RX * (TY + 2) : (TX + 2) * RY;
+constexpr int RSZ = (TX + 1) * (TY + 2) > (TX + 2) * (TY + 1) ? (TX + 1) * (TY + 2) : (TX + 2) * (TY + 1);
 constexpr int NSZ = TX * (TY + 2) > (TX + 2) * TY ? TX * (TY + 2) : (TX + 2) * TY;
+constexpr int HYP = RC + RSZ + 2 * NSZ;  // q, ratio, two cross-term arrays
 template <bool MIX>
 __host__ __device__ constexpr size_t union_bytes() {
-  return (5 * FSZ * sizeof(double)) > (QSZ + 4 * NSZ) * sizeof(typename Form<MIX>::H)
+  return (5 * FSZ * sizeof(double)) > HYP * sizeof(typename Form<MIX>::H)
              ? 5 * FSZ * sizeof(double)
-             : (QSZ + 4 * NSZ) * sizeof(typename Form<MIX>::H);
+             : HYP * sizeof(typename Form<MIX>::H);
 }
 template <bool BG, bool MIX>
 __host__ __device__ constexpr size_t smem_bytes() {
@@ -131,86 +134,99 @@ __device__ __forceinline__ double hq_global(const ST* u, const double* bg, long 
   return u[(4 + COMP) * nc + c];
 }
 
-// One hyperdiffusion pass: field kind (0 rho, 1 energy, 2 momentum, 3 B),
-// component COMP, direction DIM (src/iosmaug.c:696-810 order).
-template <bool BG, bool MIX, int KIND, int COMP, int DIM>
-__device__ __forceinline__ void hyper_pass(const T2<BG, MIX>& T, const KParams& P, const KBufs& B,
-                                           int tid, bool active, int lxo, int lyo, int gi, int gj,
-                                           double dt, double* out) {
+// (A) q of one hyperdiffusion field on the whole staged region, with the
+// reference's pads: index -1 along an axis holds the copy of index 5
+// (bc_hyperdifl), index n the stray tmp6 store of hyperdifvisc1r_parallel
+// (source table B.padsrc).  The passes of both directions read it.
+template <bool BG, bool MIX, int KIND, int COMP>
+__device__ __forceinline__ void stage_q2(const T2<BG, MIX>& T, const KParams& P, const KBufs& B,
+                                         int tid) {
   using HT = typename Form<MIX>::H;
   using ST = typename Form<MIX>::S;
-  constexpr int SX = (DIM == 0), SY = (DIM == 1);
-  constexpr int QFIELD = (KIND == 0) ? RHO : (KIND == 1) ? EN : (KIND == 2) ? M1 + COMP : B1 + COMP;
-  constexpr bool CROSS = (KIND == 2 && COMP != DIM) || (KIND == 3);
+  HT* Q = static_cast<HT*>(T.U);
   const int n0 = P.n0, n1 = P.n1;
-  const int nd = DIM == 0 ? n0 : n1;
   const long nc = P.ncell;
-  HT* Q = static_cast<HT*>(T.U);    // region-indexed (RX stride) q
-  HT* NR = Q + s2::QSZ;             // nu_r, region-indexed rows/cols of the nu area
-  HT* NL = NR + s2::NSZ;
-  HT* C3 = NL + s2::NSZ;
-  HT* C4 = C3 + s2::NSZ;
-  // nu area: tile along DIM, +-1 across; indexed (ly - oyN) * exN + (lx - oxN)
-  constexpr int exN = (DIM == 0) ? TX : TX + 2, eyN = (DIM == 0) ? TY + 2 : TY;
-  constexpr int oxN = (DIM == 0) ? HALO : HALO - 1, oyN = (DIM == 0) ? HALO - 1 : HALO;
-  // q area: full region along DIM, +-1 across; stored with region stride at region coords
-  constexpr int exQ = (DIM == 0) ? RX : TX + 2, eyQ = (DIM == 0) ? TY + 2 : RY;
-  constexpr int oxQ = (DIM == 0) ? 0 : HALO - 1, oyQ = (DIM == 0) ? HALO - 1 : 0;
-  // Q is stored in a compact array with row stride exQ
-  auto qi = [&](int lx, int ly) { return (ly - oyQ) * exQ + (lx - oxQ); };
-  auto ni = [&](int lx, int ly) { return (ly - oyN) * exN + (lx - oxN); };
-
-  // (A) q with the reference's pads at index -1 (copy of index 5,
-  // bc_hyperdifl) and index n (stray tmp6 store of hyperdifvisc1r_parallel)
-  for (int r = tid; r < exQ * eyQ; r += NTHREADS) {
-    const int lx = oxQ + r % exQ, ly = oyQ + r / exQ;
+  for (int r = tid; r < RC; r += NTHREADS) {
+    const int lx = r % RX, ly = r / RX;
     const int ci = T.x0 - HALO + lx, cj = T.y0 - HALO + ly;
-    const int a = DIM == 0 ? ci : cj, tr = DIM == 0 ? cj : ci, ntr = DIM == 0 ? n1 : n0;
+    const bool inx = ci >= 0 && ci < n0, iny = cj >= 0 && cj < n1;
     double q = 0.0;
-    if (tr >= 0 && tr < ntr) {
-      if (a >= 0 && a < nd) {
-        q = hq_at<BG, MIX, KIND, COMP>(T, ly * RX + lx);
-      } else if (a == -1) {
-        q = hq_at<BG, MIX, KIND, COMP>(T, (ly + 6 * SY) * RX + lx + 6 * SX);
-      } else if (a == nd) {
-        const int src = B.padsrc[DIM][tr];
+    if (inx && iny) {
+      q = hq_at<BG, MIX, KIND, COMP>(T, r);
+    } else if (iny) {
+      if (ci == -1) {
+        q = hq_at<BG, MIX, KIND, COMP>(T, r + 6);
+      } else if (ci == n0) {
+        const int src = B.padsrc[0][cj];
+        if (src >= 0) q = hq_global<ST, KIND, COMP>(static_cast<const ST*>(B.uin), B.bg, nc, src);
+      }
+    } else if (inx) {
+      if (cj == -1) {
+        q = hq_at<BG, MIX, KIND, COMP>(T, r + 6 * RX);
+      } else if (cj == n1) {
+        const int src = B.padsrc[1][ci];
         if (src >= 0) q = hq_global<ST, KIND, COMP>(static_cast<const ST*>(B.uin), B.bg, nc, src);
       }
     }
     Q[r] = (HT)q;
   }
   __syncthreads();
-  // (B) nu_r, nu_l (hyperdifvisc2-4): third differences D3 over faces
-  // i-2..i+1, first differences D1 over faces i-3..i+2
+}
+
+// One hyperdiffusion pass on staged q: field kind (0 rho, 1 energy,
+// 2 momentum, 3 B), component COMP, direction DIM.
+//
+// nu_r and nu_l (hyperdifvisc2-4) are ratios of windowed maxima of the third
+// differences D3 and first differences D1 of q:
+//   nu_r(i) = dl(i) cmax chyp max D3(i-1..i+1) / max D1(i-2..i+2)
+//   nu_l(i) = dl(i) cmax chyp max D3(i-2..i)   / max D1(i-3..i+1)
+// (0 where the denominator is 0, and 0 outside [2, n-3] in every
+// dimension).  The windows of nu_l(i) are those of nu_r(i-1), so one ratio
+// R(i) = max D3 / max D1 per cell serves both: nu_r(i) = c(i) R(i),
+// nu_l(i) = c(i) R(i-1).
+template <bool BG, bool MIX, int KIND, int COMP, int DIM>
+__device__ __forceinline__ void hyper_pass(const T2<BG, MIX>& T, const KParams& P, const KBufs& B,
+                                           int tid, bool active, int lxo, int lyo, int gi, int gj,
+                                           double dt, double* out) {
+  using HT = typename Form<MIX>::H;
+  constexpr int SX = (DIM == 0), SY = (DIM == 1);
+  constexpr int QFIELD = (KIND == 0) ? RHO : (KIND == 1) ? EN : (KIND == 2) ? M1 + COMP : B1 + COMP;
+  constexpr bool CROSS = (KIND == 2 && COMP != DIM) || (KIND == 3);
+  const int n0 = P.n0, n1 = P.n1;
+  const int nd = DIM == 0 ? n0 : n1;
+  const HT* Q = static_cast<const HT*>(T.U);  // region-indexed q
+  HT* RR = static_cast<HT*>(T.U) + RC;         // ratio area
+  HT* C3 = RR + s2::RSZ;                       // cross-term arrays (nu area)
+  HT* C4 = C3 + s2::NSZ;
+  constexpr int SQ = DIM == 0 ? 1 : RX;        // stride along DIM in Q
+  // ratio area: the tile along DIM extended by one cell below, the tile
+  // across (+-1 when cross terms need it)
+  constexpr int exR = DIM == 0 ? TX + 1 : (CROSS ? TX + 2 : TX);
+  constexpr int eyR = DIM == 0 ? (CROSS ? TY + 2 : TY) : TY + 1;
+  constexpr int oxR = DIM == 0 ? HALO - 1 : (CROSS ? HALO - 1 : HALO);
+  constexpr int oyR = DIM == 0 ? (CROSS ? HALO - 1 : HALO) : HALO - 1;
+  constexpr int SR = DIM == 0 ? 1 : exR;       // stride along DIM in RR
+  // nu area: the tile along DIM, +-1 across
+  constexpr int exN = (DIM == 0) ? TX : TX + 2, eyN = (DIM == 0) ? TY + 2 : TY;
+  constexpr int oxN = (DIM == 0) ? HALO : HALO - 1, oyN = (DIM == 0) ? HALO - 1 : HALO;
+  auto ri = [&](int lx, int ly) { return (ly - oyR) * exR + (lx - oxR); };
+  auto ni = [&](int lx, int ly) { return (ly - oyN) * exN + (lx - oxN); };
   const HT coef = (HT)(B.cmax_in[DIM] * P.chyp[QFIELD]);
-  for (int r = tid; r < exN * eyN; r += NTHREADS) {
-    const int lx = oxN + r % exN, ly = oyN + r / exN;
-    const int ci = T.x0 - HALO + lx, cj = T.y0 - HALO + ly;
-    HT nur = 0, nul = 0;
-    if (ci >= 2 && ci <= n0 - 3 && cj >= 2 && cj <= n1 - 3) {
-      const int q0 = qi(lx, ly);
-      constexpr int st = DIM == 0 ? 1 : exQ;
-      HT q[7];
+
+  // (B) R = max D3(i-1..i+1) / max D1(i-2..i+2) from q(i-2..i+3)
+  for (int r = tid; r < exR * eyR; r += NTHREADS) {
+    const int lx = oxR + r % exR, ly = oyR + r / exR;
+    const int l = ly * RX + lx;
+    HT q[6];
 #pragma unroll
-      for (int s = 0; s < 7; s++) q[s] = Q[q0 + (s - 3) * st];
-      HT d1[6], d3[4];
+    for (int s = 0; s < 6; s++) q[s] = Q[l + (s - 2) * SQ];
+    HT t4 = 0, t5 = 0;
 #pragma unroll
-      for (int k = 0; k < 6; k++) d1[k] = fabs(q[k + 1] - q[k]);
+    for (int k = 0; k < 3; k++)
+      t4 = hmax0(t4, (HT)fabs((HT)3 * (q[k + 2] - q[k + 1]) - (q[k + 3] - q[k])));
 #pragma unroll
-      for (int k = 0; k < 4; k++) d3[k] = fabs((HT)3 * (q[k + 2] - q[k + 1]) - (q[k + 3] - q[k]));
-      HT t4r = 0, t5r = 0, t4l = 0, t5l = 0;
-      t4r = hmax0(hmax0(hmax0(t4r, d3[1]), d3[2]), d3[3]);
-      t4l = hmax0(hmax0(hmax0(t4l, d3[0]), d3[1]), d3[2]);
-#pragma unroll
-      for (int k = 1; k < 6; k++) t5r = hmax0(t5r, d1[k]);
-#pragma unroll
-      for (int k = 0; k < 5; k++) t5l = hmax0(t5l, d1[k]);
-      const HT c = (HT)(DIM == 0 ? T.dl0[lx] : T.dl1[ly]) * coef;
-      if (t5r > 0) nur = c * t4r / t5r;
-      if (t5l > 0) nul = c * t4l / t5l;
-    }
-    NR[r] = nur;
-    NL[r] = nul;
+    for (int k = 0; k < 5; k++) t5 = hmax0(t5, (HT)fabs(q[k + 1] - q[k]));
+    RR[r] = (t5 > 0) ? t4 / t5 : (HT)0;
   }
   __syncthreads();
   // (C) cross-term arrays (hyperdifmomsourcene2-4 / hyperdifbsourcene1b-4)
@@ -221,13 +237,16 @@ __device__ __forceinline__ void hyper_pass(const T2<BG, MIX>& T, const KParams& 
       HT c3 = 0, c4 = 0;
       if (ci > 0 && ci < n0 - 1 && cj > 0 && cj < n1 - 1) {
         const int a = DIM == 0 ? ci : cj;
-        const int q0 = qi(lx, ly);
-        constexpr int st = DIM == 0 ? 1 : exQ;
-        // grad13n along DIM of q
-        HT g = ((Q[q0 + st] - Q[q0 - st]) * (HT)(DIM == 0 ? T.rd0[lx] : T.rd1[ly])) * (HT)0.5;
-        if ((P.bt[DIM] != 0) && zero1n(a, nd)) g = 0;
-        const HT nsum = NR[r] + NL[r];
         const int l = ly * RX + lx;
+        // grad13n along DIM of q
+        HT g = ((Q[l + SQ] - Q[l - SQ]) * (HT)(DIM == 0 ? T.rd0[lx] : T.rd1[ly])) * (HT)0.5;
+        if ((P.bt[DIM] != 0) && zero1n(a, nd)) g = 0;
+        HT nsum = 0;
+        if (ci >= 2 && ci <= n0 - 3 && cj >= 2 && cj <= n1 - 3) {
+          const int rr = ri(lx, ly);
+          const HT c = (HT)(DIM == 0 ? T.dl0[lx] : T.dl1[ly]) * coef;
+          nsum = c * RR[rr] + c * RR[rr - SR];
+        }
         if (KIND == 2) {
           const HT tau = (g * nsum) * (HT)0.25;
           c3 = (HT)(T.v(RHO, l) + T.v(RHOB, l)) * tau;
@@ -243,19 +262,19 @@ __device__ __forceinline__ void hyper_pass(const T2<BG, MIX>& T, const KParams& 
     }
     __syncthreads();
   }
-  // (D) sources at the tile cells
+  // (D) sources at the tile cells (all inside [2, n-3])
   if (active) {
     const int a = DIM == 0 ? gi : gj;
-    const int q0 = qi(lxo, lyo);
-    constexpr int st = DIM == 0 ? 1 : exQ;
+    const int l = lyo * RX + lxo;
+    const int rr = ri(lxo, lyo);
     const int nidx = ni(lxo, lyo);
-    const HT nur = NR[nidx], nul = NL[nidx];
+    const HT c = (HT)(DIM == 0 ? T.dl0[lxo] : T.dl1[lyo]) * coef;
+    const HT nur = c * RR[rr], nul = c * RR[rr - SR];
     const HT rdl = (HT)(DIM == 0 ? T.rd0[lxo] : T.rd1[lyo]);
-    const HT qc = Q[q0], qp = Q[q0 + st], qm = Q[q0 - st];
+    const HT qc = Q[l], qp = Q[l + SQ], qm = Q[l - SQ];
     HT gr = (qp - qc) * rdl;   // grad1r3n
     HT gl = (qc - qm) * rdl;   // grad1l3n
     if ((P.bt[DIM] != 0) && zero1n(a, nd)) { gr = 0; gl = 0; }
-    const int l = lyo * RX + lxo;
     constexpr int SL = SX + SY * RX;  // region stride along DIM
     if (KIND == 0) {
       out[RHO] = out[RHO] + dt * (double)((nur * gr - nul * gl) * rdl);
@@ -480,10 +499,14 @@ __device__ __forceinline__ void stage2d_body(const KParams& P, const KBufs& B, i
   // ---- hyperdiffusion, in the driver's order -------------------------------
   if (P.hyperdif == 1) {
 #define HP(K, C, D) hyper_pass<BG, MIX, K, C, D>(T, P, B, tid, active, lxo, lyo, gi, gj, dt, out)
-    HP(0, 0, 0); HP(0, 0, 1);
-    HP(1, 0, 0); HP(1, 0, 1);
-    HP(2, 0, 0); HP(2, 1, 0); HP(2, 0, 1); HP(2, 1, 1);
-    HP(3, 1, 0); HP(3, 0, 1);
+#define SQ(K, C) stage_q2<BG, MIX, K, C>(T, P, B, tid)
+    SQ(0, 0); HP(0, 0, 0); HP(0, 0, 1);
+    SQ(1, 0); HP(1, 0, 0); HP(1, 0, 1);
+    SQ(2, 0); HP(2, 0, 0); HP(2, 0, 1);
+    SQ(2, 1); HP(2, 1, 0); HP(2, 1, 1);
+    SQ(3, 1); HP(3, 1, 0);
+    SQ(3, 0); HP(3, 0, 1);
+#undef SQ
 #undef HP
   }
 

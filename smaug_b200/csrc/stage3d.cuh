@@ -25,8 +25,10 @@
 // the per-axis metric, and one union of phase scratch:
 //   flux phase:  7 flux arrays + 3 velocity arrays on the tile +-2 along the
 //                direction
-//   hyperdiffusion phase: nu_r, nu_l and two cross-term arrays on the tile
-//                +-1 across the direction.
+//   hyperdiffusion phase: q of one field on the box (shared by the passes
+//                of all directions), the nu ratio on the tile +-1 across the
+//                direction extended by one cell along it, two cross-term
+//                arrays on the tile +-1 across the direction.
 #pragma once
 
 // (included inside namespace smaug)
@@ -43,7 +45,10 @@ __host__ __device__ constexpr int max3(int a, int b, int c) {
 constexpr int FA = max3((T0 + 4) * T1 * T2, T0 * (T1 + 4) * T2, T0 * T1 * (T2 + 4));
 constexpr int NA = max3(T0 * (T1 + 2) * (T2 + 2), (T0 + 2) * T1 * (T2 + 2), (T0 + 2) * (T1 + 2) * T2);
 constexpr int FLUX_SCR = 10 * FA;
-constexpr int HYP_SCR = BC + 4 * NA;
+// ratio area: the nu area extended by one cell below along the direction
+constexpr int RA = max3((T0 + 1) * (T1 + 2) * (T2 + 2), (T0 + 2) * (T1 + 1) * (T2 + 2),
+                        (T0 + 2) * (T1 + 2) * (T2 + 1));
+constexpr int HYP_SCR = BC + RA + 2 * NA;
 constexpr int NMET = 2 * (BX + BY + BZ);
 template <bool MIX>
 __host__ __device__ constexpr size_t union_bytes() {
@@ -166,48 +171,40 @@ __device__ __forceinline__ void hyper_pass3(const Box3& X, const KParams& P, con
   constexpr int G1 = s3::H - ((CROSS && DIM != 1) ? 1 : 0);
   constexpr int G2 = s3::H - ((CROSS && DIM != 2) ? 1 : 0);
   constexpr int NAREA = E0 * E1 * E2;
+  // ratio area: the nu area extended by one cell below along DIM
+  constexpr int RE0 = E0 + (DIM == 0), RE1 = E1 + (DIM == 1), RE2 = E2 + (DIM == 2);
+  constexpr int RG0 = G0 - (DIM == 0), RG1 = G1 - (DIM == 1), RG2 = G2 - (DIM == 2);
+  constexpr int RAREA = RE0 * RE1 * RE2;
+  constexpr int RS = DIM == 0 ? 1 : (DIM == 1 ? RE0 : RE0 * RE1);  // stride along DIM in R
   using HT = typename Form<MIX>::H;
   using ST = typename Form<MIX>::S;
   const ST* u = static_cast<const ST*>(B.uin);
   const int n[3] = {P.n0, P.n1, P.n2};
   const long nc = P.ncell;
   const HT* Q = static_cast<const HT*>(X.U);
-  HT* NR = static_cast<HT*>(X.U) + s3::BC;
-  HT* NL = NR + s3::NA;
-  HT* C3 = NL + s3::NA;
+  HT* RR = static_cast<HT*>(X.U) + s3::BC;
+  HT* C3 = RR + s3::RA;
   HT* C4 = C3 + s3::NA;
   auto aidx = [&](int lx, int ly, int lz) { return ((lz - G2) * E1 + (ly - G1)) * E0 + (lx - G0); };
+  auto ridx = [&](int lx, int ly, int lz) { return ((lz - RG2) * RE1 + (ly - RG1)) * RE0 + (lx - RG0); };
 
-  // (B) nu_r, nu_l (hyperdifvisc2-4)
+  // (B) nu_r(i) = c(i) R(i), nu_l(i) = c(i) R(i-1) with
+  // R(i) = max D3(i-1..i+1) / max D1(i-2..i+2) (hyperdifvisc2-4; the windows
+  // of nu_l(i) are those of nu_r(i-1)); 0 where the denominator is 0
   const HT coef = (HT)(B.cmax_in[DIM] * P.chyp[QFIELD]);
-  for (int r = tid; r < NAREA; r += s3::NT) {
-    const int lx = G0 + r % E0, ly = G1 + (r / E0) % E1, lz = G2 + r / (E0 * E1);
-    const int g0 = X.o[0] + lx, g1 = X.o[1] + ly, g2 = X.o[2] + lz;
-    HT nur = 0, nul = 0;
-    if (g0 >= 2 && g0 <= n[0] - 3 && g1 >= 2 && g1 <= n[1] - 3 && g2 >= 2 && g2 <= n[2] - 3) {
-      const int q0 = (lz * s3::BY + ly) * s3::BX + lx;
-      HT q[7];
+  for (int r = tid; r < RAREA; r += s3::NT) {
+    const int lx = RG0 + r % RE0, ly = RG1 + (r / RE0) % RE1, lz = RG2 + r / (RE0 * RE1);
+    const int q0 = (lz * s3::BY + ly) * s3::BX + lx;
+    HT q[6];
 #pragma unroll
-      for (int s = 0; s < 7; s++) q[s] = Q[q0 + (s - 3) * SD];
-      HT d1[6], d3[4];
+    for (int s = 0; s < 6; s++) q[s] = Q[q0 + (s - 2) * SD];
+    HT t4 = 0, t5 = 0;
 #pragma unroll
-      for (int k = 0; k < 6; k++) d1[k] = fabs(q[k + 1] - q[k]);
+    for (int k = 0; k < 3; k++)
+      t4 = hmax0(t4, (HT)fabs((HT)3 * (q[k + 2] - q[k + 1]) - (q[k + 3] - q[k])));
 #pragma unroll
-      for (int k = 0; k < 4; k++) d3[k] = fabs((HT)3 * (q[k + 2] - q[k + 1]) - (q[k + 3] - q[k]));
-      HT t4r = 0, t5r = 0, t4l = 0, t5l = 0;
-      t4r = hmax0(hmax0(hmax0(t4r, d3[1]), d3[2]), d3[3]);
-      t4l = hmax0(hmax0(hmax0(t4l, d3[0]), d3[1]), d3[2]);
-#pragma unroll
-      for (int k = 1; k < 6; k++) t5r = hmax0(t5r, d1[k]);
-#pragma unroll
-      for (int k = 0; k < 5; k++) t5l = hmax0(t5l, d1[k]);
-      const int la = DIM == 0 ? lx : (DIM == 1 ? ly : lz);
-      const HT c = (HT)X.dl[DIM][la] * coef;
-      if (t5r > 0) nur = c * t4r / t5r;
-      if (t5l > 0) nul = c * t4l / t5l;
-    }
-    NR[r] = nur;
-    NL[r] = nul;
+    for (int k = 0; k < 5; k++) t5 = hmax0(t5, (HT)fabs(q[k + 1] - q[k]));
+    RR[r] = (t5 > 0) ? t4 / t5 : (HT)0;
   }
   __syncthreads();
   // (C) cross-term arrays (hyperdifmomsourcene2-4 / hyperdifbsourcene1b-4)
@@ -222,7 +219,13 @@ __device__ __forceinline__ void hyper_pass3(const Box3& X, const KParams& P, con
         // grad13n along DIM of q
         HT gq = ((Q[q0 + SD] - Q[q0 - SD]) * (HT)X.rd[DIM][la]) * (HT)0.5;
         if ((P.bt[DIM] != 0) && zero1n(g[DIM], n[DIM])) gq = 0;
-        const HT nsum = NR[r] + NL[r];
+        HT nsum = 0;
+        if (g[0] >= 2 && g[0] <= n[0] - 3 && g[1] >= 2 && g[1] <= n[1] - 3 && g[2] >= 2 &&
+            g[2] <= n[2] - 3) {
+          const int rr = ridx(lx, ly, lz);
+          const HT cc = (HT)X.dl[DIM][la] * coef;
+          nsum = cc * RR[rr] + cc * RR[rr - RS];
+        }
         const long c = ((long)g[2] * n[1] + g[1]) * n[0] + g[0];
         if (KIND == 2) {
           const HT tau = (gq * nsum) * (HT)0.25;
@@ -244,7 +247,9 @@ __device__ __forceinline__ void hyper_pass3(const Box3& X, const KParams& P, con
     const int la = lt[DIM];
     const int q0 = (lt[2] * s3::BY + lt[1]) * s3::BX + lt[0];
     const int nidx = aidx(lt[0], lt[1], lt[2]);
-    const HT nur = NR[nidx], nul = NL[nidx];
+    const int rr = ridx(lt[0], lt[1], lt[2]);
+    const HT cc = (HT)X.dl[DIM][la] * coef;
+    const HT nur = cc * RR[rr], nul = cc * RR[rr - RS];
     const HT rdl = (HT)X.rd[DIM][la];
     const HT qc = Q[q0], qp = Q[q0 + SD], qm = Q[q0 - SD];
     HT gr = (qp - qc) * rdl;  // grad1r3n
