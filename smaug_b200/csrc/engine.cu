@@ -186,6 +186,12 @@ static int validate(const smaug_params_t* p) {
   if (p->ndim != 2 && p->ndim != 3) return set_error(SMAUG_E_INVALID, "ndim must be 2 or 3 (got %d)", p->ndim);
   for (int d = 0; d < p->ndim; d++)
     if (p->n[d] < 8) return set_error(SMAUG_E_INVALID, "n[%d]=%d: need at least 4 interior cells", d, p->n[d]);
+  {
+    long long cells = 1;
+    for (int d = 0; d < p->ndim; d++) cells *= p->n[d];
+    if (cells >= (1LL << 31) - 2)
+      return set_error(SMAUG_E_UNSUPPORTED, "%lld cells: grids are limited to 2^31-2 cells", cells);
+  }
   if (p->integrator != SMAUG_INT_EULER && p->integrator != SMAUG_INT_RK4)
     return set_error(SMAUG_E_INVALID, "unknown integrator %d", p->integrator);
   if (p->precision != SMAUG_PREC_FP64 && p->precision != SMAUG_PREC_MIXED)

@@ -58,7 +58,7 @@ __host__ __device__ constexpr size_t union_bytes() {
 }
 template <bool MIX>
 __host__ __device__ constexpr size_t smem_bytes() {
-  return sizeof(double) * (BC + NMET) + union_bytes<MIX>();
+  return sizeof(double) * (BC + NMET) + union_bytes<MIX>() + sizeof(int) * BC;
 }
 __host__ __device__ constexpr int tdim(int d) { return d == 0 ? T0 : (d == 1 ? T1 : T2); }
 __host__ __device__ constexpr int bstride(int d) { return d == 0 ? 1 : (d == 1 ? BS1 : BS2); }
@@ -69,6 +69,7 @@ struct Box3 {
   double* dl[3];   // cell widths over the box extent of each axis
   double* rd[3];   // reciprocals
   void* U;         // union scratch
+  int* C;          // [BC] q source code per box cell (box_code)
   int o[3];        // global coordinate of box index 0 per axis
 };
 
@@ -106,52 +107,61 @@ __device__ __forceinline__ void stage_q(const Box3& X, const KParams& P, const K
   const ST* u = static_cast<const ST*>(B.uin);
   HT* Q = static_cast<HT*>(X.U);
   const long nc = P.ncell;
-  const int n[3] = {P.n0, P.n1, P.n2};
   for (int r = tid; r < s3::BC; r += s3::NT) {
-    const int lx = r % s3::BX, ly = (r / s3::BX) % s3::BY, lz = r / s3::BS2;
-    const int ox = outside(lx, s3::T0), oy = outside(ly, s3::T1), oz = outside(lz, s3::T2);
-    const int nbig = (ox > 1) + (oy > 1) + (oz > 1);
+    const int code = X.C[r];
     double q = 0.0;
-    if (nbig <= 1) {
-      int g[3] = {X.o[0] + lx, X.o[1] + ly, X.o[2] + lz};
-      int nout = 0, ax = -1;
+    if (code >= 0) {
+      const long c = code;
+      if (KIND == 0) {
+        q = __ldg(u + c);
+      } else if (KIND == 3) {
+        q = __ldg(u + (B3 + COMP) * nc + c);
+      } else if (KIND == 2) {
+        q = (double)__ldg(u + (M3 + COMP) * nc + c) * X.R[r];
+      } else {
+        double m2 = 0, b2 = 0;
 #pragma unroll
-      for (int a = 0; a < 3; a++)
-        if (g[a] < 0 || g[a] >= n[a]) { nout++; ax = a; }
-      if (nout == 0) {
-        const long c = ((long)g[2] * n[1] + g[1]) * n[0] + g[0];
-        if (KIND == 0) {
-          q = __ldg(u + c);
-        } else if (KIND == 3) {
-          q = __ldg(u + (B3 + COMP) * nc + c);
-        } else if (KIND == 2) {
-          q = (double)__ldg(u + (M3 + COMP) * nc + c) * X.R[r];
-        } else {
-          double m2 = 0, b2 = 0;
-#pragma unroll
-          for (int a = 0; a < 3; a++) {
-            const double m = __ldg(u + (M3 + a) * nc + c), b = __ldg(u + (B3 + a) * nc + c);
-            m2 += m * m;
-            b2 += b * b;
-          }
-          q = (double)__ldg(u + E3 * nc + c) - 0.5 * (b2 + m2 * X.R[r]);
+        for (int a = 0; a < 3; a++) {
+          const double m = __ldg(u + (M3 + a) * nc + c), b = __ldg(u + (B3 + a) * nc + c);
+          m2 += m * m;
+          b2 += b * b;
         }
-      } else if (nout == 1) {
-        if (g[ax] == -1) {
-          g[ax] = 5;
-          const long c = ((long)g[2] * n[1] + g[1]) * n[0] + g[0];
-          q = hq3_global<ST, KIND, COMP>(u, B, nc, c);
-        } else if (g[ax] == n[ax]) {
-          // across index of the pad table: the other two coordinates, lower axis fastest
-          const int a1 = ax == 0 ? 1 : 0, a2 = ax == 2 ? 1 : 2;
-          const int src = B.padsrc[ax][(long)g[a2] * n[a1] + g[a1]];
-          if (src >= 0) q = hq3_global<ST, KIND, COMP>(u, B, nc, src);
-        }
+        q = (double)__ldg(u + E3 * nc + c) - 0.5 * (b2 + m2 * X.R[r]);
       }
+    } else if (code <= -2) {
+      q = hq3_global<ST, KIND, COMP>(u, B, nc, (long)(-2 - code));
     }
     Q[r] = (HT)q;
   }
   __syncthreads();
+}
+
+// Source code of box cell r for the q stagings (computed once per block):
+// the cell index when the cell is in the grid and read by some pass, -2 - src
+// for a pad (index -1 along an axis: the cell with that coordinate 5,
+// bc_hyperdifl; index n: the stray tmp6 store of hyperdifvisc1r_parallel,
+// source table B.padsrc), -1 for a zero.  The passes read the cells within 1
+// of the tile on all axes but one and within 3 on that one.
+__device__ __forceinline__ int box_code(const Box3& X, const KParams& P, const KBufs& B, int lx, int ly,
+                                        int lz) {
+  const int ox = outside(lx, s3::T0), oy = outside(ly, s3::T1), oz = outside(lz, s3::T2);
+  if ((ox > 1) + (oy > 1) + (oz > 1) > 1) return -1;
+  const int n0 = P.n0, n1 = P.n1, n2 = P.n2;
+  const int g0 = X.o[0] + lx, g1 = X.o[1] + ly, g2 = X.o[2] + lz;
+  const bool i0 = g0 >= 0 && g0 < n0, i1 = g1 >= 0 && g1 < n1, i2 = g2 >= 0 && g2 < n2;
+  if (i0 && i1 && i2) return (int)(((long)g2 * n1 + g1) * n0 + g0);
+  int src = -1;
+  if (!i0 && i1 && i2) {
+    if (g0 == -1) src = (int)(((long)g2 * n1 + g1) * n0 + 5);
+    else if (g0 == n0) src = B.padsrc[0][(long)g2 * n1 + g1];
+  } else if (i0 && !i1 && i2) {
+    if (g1 == -1) src = (int)(((long)g2 * n1 + 5) * n0 + g0);
+    else if (g1 == n1) src = B.padsrc[1][(long)g2 * n0 + g0];
+  } else if (i0 && i1 && !i2) {
+    if (g2 == -1) src = (int)(((long)5 * n1 + g1) * n0 + g0);
+    else if (g2 == n2) src = B.padsrc[2][(long)g1 * n0 + g0];
+  }
+  return src >= 0 ? -2 - src : -1;
 }
 
 // One hyperdiffusion pass on staged q: field kind (0 rho, 1 energy,
@@ -421,6 +431,7 @@ __global__ void __launch_bounds__(s3::NT, 3) stage3d_fast(const KParams P, const
   X.rd[1] = X.rd[0] + s3::BX;
   X.rd[2] = X.rd[1] + s3::BY;
   X.U = X.rd[2] + s3::BZ;
+  X.C = reinterpret_cast<int*>(reinterpret_cast<unsigned char*>(X.U) + s3::union_bytes<MIX>());
   const int tid = threadIdx.x;
   const int tx = tid % s3::T0, ty = (tid / s3::T0) % s3::T1, tz = tid / (s3::T0 * s3::T1);
   const int n[3] = {P.n0, P.n1, P.n2};
@@ -439,6 +450,7 @@ __global__ void __launch_bounds__(s3::NT, 3) stage3d_fast(const KParams P, const
       rinv = 1.0 / ((double)__ldg(u + c) + __ldg(B.bg + GRB * nc + c));
     }
     X.R[r] = rinv;
+    X.C[r] = box_code(X, P, B, lx, ly, lz);
   }
   for (int r = tid; r < s3::BX + s3::BY + s3::BZ; r += s3::NT) {
     const int a = r < s3::BX ? 0 : (r < s3::BX + s3::BY ? 1 : 2);
