@@ -13,7 +13,7 @@ namespace smaug {
 #include "stage2d.cuh"
 
 template <int MODE, bool MIX>
-__global__ void __launch_bounds__(NTHREADS, 3)
+__global__ void __launch_bounds__(NTHREADS, SMAUG_MINB2D)
     stage2d_batch(const KParams* __restrict__ Ks, const KBufs* __restrict__ Bs,
                   const int4* __restrict__ tiles, int ntiles) {
   for (int it = blockIdx.x; it < ntiles; it += gridDim.x) {

@@ -14,8 +14,19 @@ namespace smaug {
 // ---------------------------------------------------------------------------
 // kernel parameters
 // ---------------------------------------------------------------------------
-constexpr int TX = 32;             // tile width (x, fastest)
-constexpr int TY = 8;              // tile height
+// 2D tile shape and the minimum resident blocks per SM of the 2D kernels
+// (compile-time; -DSMAUG_TX=.. -DSMAUG_TY=.. -DSMAUG_MINB2D=.. select others)
+#ifndef SMAUG_TX
+#define SMAUG_TX 32
+#endif
+#ifndef SMAUG_TY
+#define SMAUG_TY 8
+#endif
+#ifndef SMAUG_MINB2D
+#define SMAUG_MINB2D 4
+#endif
+constexpr int TX = SMAUG_TX;       // tile width (x, fastest)
+constexpr int TY = SMAUG_TY;       // tile height
 constexpr int HALO = 3;            // stencil radius of the hyperdiffusion windows
 constexpr int RX = TX + 2 * HALO;  // staged region
 constexpr int RY = TY + 2 * HALO;

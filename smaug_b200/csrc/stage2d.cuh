@@ -597,7 +597,7 @@ __device__ __forceinline__ void stage2d_body(const KParams& P, const KBufs& B, i
 }
 
 template <int MODE, bool BG, bool MIX>
-__global__ void __launch_bounds__(NTHREADS, 3) stage2d_fast(const KParams P, const KBufs B) {
+__global__ void __launch_bounds__(NTHREADS, SMAUG_MINB2D) stage2d_fast(const KParams P, const KBufs B) {
   stage2d_body<MODE, BG, MIX>(P, B, blockIdx.x, blockIdx.y);
 }
 
