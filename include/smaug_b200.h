@@ -198,6 +198,27 @@ int smaug_batch_get_time(smaug_batch_t b, int32_t run, int64_t* it, double* t, d
 int smaug_batch_launch_shape(smaug_batch_t b, int32_t* grid, int32_t* candidates, float* ms);
 int smaug_batch_destroy(smaug_batch_t b);
 
+/* ---- adjoint of one RK4 step (2D, FP64, dt held fixed) -------------------
+ * No counterpart in the reference (which has no derivatives).  The step is
+ * u -> U' = RK4 step of G(u) (G: ghost fill) with dt = p->dt fixed
+ * (p->moddton must be 0), the hyperdiffusion coefficient's maxima and the CFL
+ * maxima differentiated through the cells that attain them.  States are
+ * DEVICE arrays of the 2D evolved fields [6][n1*n0] in reference layout; the
+ * background fields are taken from w at create.  Driver parameters theta =
+ * (amplitude, period, centre along dim 1). */
+typedef struct smaug_adj_s* smaug_adj_t;
+
+int smaug_adj_create(const smaug_params_t* p, const double* w, const double* pos, smaug_adj_t* out);
+/* theta of the driver term (overrides p's drv_amp, drv_period, drv_x0[1]) */
+int smaug_adj_set_driver(smaug_adj_t a, double amp, double period, double x0);
+/* u_next = step(u) at time t; enqueued on `stream` */
+int smaug_adj_forward(smaug_adj_t a, const double* u, double* u_next, double t, void* stream);
+/* ubar = (dU'/du)^T ubar_next, thbar[3] = (dU'/dtheta)^T ubar_next (device
+   arrays, overwritten); recomputes the step's stages; enqueued on `stream` */
+int smaug_adj_backward(smaug_adj_t a, const double* u, const double* ubar_next, double* ubar,
+                       double* thbar, double t, void* stream);
+int smaug_adj_destroy(smaug_adj_t a);
+
 /* Message of the calling thread's last failure ("" if none). */
 const char* smaug_last_error(void);
 

@@ -23,6 +23,8 @@ EXPORTS = [
     "smaug_set_stream", "smaug_euler_step_noalloc", "smaug_batch_create", "smaug_batch_step",
     "smaug_batch_get_state", "smaug_batch_get_time", "smaug_batch_launch_shape",
     "smaug_batch_destroy", "smaug_batch_step_async", "smaug_batch_sync", "smaug_batch_set_stream",
+    "smaug_adj_create", "smaug_adj_set_driver", "smaug_adj_forward", "smaug_adj_backward",
+    "smaug_adj_destroy",
 ]
 
 ERRORS = {1: "invalid", 2: "cuda", 3: "nomem", 4: "io", 5: "format", 6: "unsupported",
@@ -82,6 +84,11 @@ def lib():
                                                ctypes.POINTER(ctypes.c_int32),
                                                ctypes.POINTER(ctypes.c_float)]
         L.smaug_batch_destroy.argtypes = [vp]
+        L.smaug_adj_create.argtypes = [vp, dp, dp, ctypes.POINTER(vp)]
+        L.smaug_adj_set_driver.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_double]
+        L.smaug_adj_forward.argtypes = [vp, vp, vp, ctypes.c_double, vp]
+        L.smaug_adj_backward.argtypes = [vp, vp, vp, vp, vp, ctypes.c_double, vp]
+        L.smaug_adj_destroy.argtypes = [vp]
         _lib = L
     return _lib
 
