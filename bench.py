@@ -28,6 +28,10 @@ Orszag-Tang and stratified driven slabs) advanced by one batch (one launch per
 stage for all runs, CUDA-graph cycles, autotuned launch shape), against the
 same runs stepped one by one; mixed precision unless --precision fp64.
 
+--workload adjoint: the driver-parameter gradient of a 400-step loss on a
+256 x 512 stratified slab through the hand-written adjoint (checkpoints every
+20 steps): adjoint-to-forward cost ratio and the finite-difference check.
+
 --impl reference: the reference has no CPU solver (every routine is a CUDA
 kernel), so the CPU baseline is the oracle, the FP64 restatement of the
 reference's kernels (oracle/), run with all host threads on a bounded
@@ -258,6 +262,112 @@ def ensemble_main(args):
     print(json.dumps(line), flush=True)
 
 
+def make_slab(nx=256, nz=512, seed=11):
+    """2D stratified slab 256 (x) x 512 (z), 2 x 6 Mm, vertical dim 0, seeded
+    FP32 v_z perturbation (sigma 10 m/s, Gaussian-smoothed over 3 cells),
+    Gaussian driver (200 m/s, 30 s, x0 = 1 Mm, z = 0.1 Mm, sigma 0.2 Mm)."""
+    from smaug_b200 import ic, params as P
+    w, pos, dx = ic.stratified(nz=nz, nx=nx, seed=seed, vz_sigma=10.0)
+    p = P.make_params(ndim=2, n=(nz + 4, nx + 4, 1), dx=dx, courant=0.3, dtmax=1.0,
+                      integrator=P.INT_RK4, g=(-274.0, 0.0),
+                      boundtype=(P.BC_CONTCD4, P.BC_PERIODIC), driver=P.DRIVER_GAUSS,
+                      drv_amp=200.0, drv_period=30.0, drv_x0=(0.1e6, 1.0e6),
+                      drv_sigma=(0.2e6, 0.2e6))
+    return p, w, pos
+
+
+def adjoint_main(args):
+    """--workload adjoint: gradient of sum_n sum_x (v_z(z = 3 Mm) - target)^2
+    over 400 RK4 steps with respect to the driver (amplitude, period, x0),
+    through the hand-written adjoint with checkpoints every 20 steps; the
+    target comes from a forward run with seed-shifted parameters.  Reports the
+    forward and forward+backward times (CUDA events), their ratio, and the
+    central finite-difference check (h = 1e-4 relative) of every component."""
+    import numpy as np
+    import torch
+    from smaug_b200 import engine, params as P
+    from smaug_b200.adjoint import StepAdjoint, rollout
+    nsteps = args.adj_steps
+    p, w, pos = make_slab()
+    e = engine.Engine(p, w, pos)
+    e.step(1)
+    dt = e.time()[2]
+    e.close()
+    q = P.SmaugParams.from_buffer_copy(p)
+    q.moddton = 0
+    q.dt = 0.5 * dt
+    sa = StepAdjoint(q, w, pos)
+    u0 = torch.tensor(w[:6], dtype=torch.float64, device="cuda").contiguous()
+    kz = int(np.argmin(np.abs(pos[0][0] - args.obs_z)))
+    rhob = torch.tensor(w[7], device="cuda", dtype=torch.float64)
+    theta0 = torch.tensor([200.0, 30.0, 1.0e6], dtype=torch.float64)
+    rng = np.random.default_rng(12)
+    shift = torch.tensor(1.0 + 0.05 * rng.standard_normal(3), dtype=torch.float64)
+
+    def vz_row(u):
+        return u[1, :, kz] / (u[0, :, kz] + rhob[:, kz])
+
+    with torch.no_grad():
+        sa.set_driver(*(theta0 * shift).tolist())
+        target, u = [], u0
+        for n in range(nsteps):
+            u = sa.forward(u, n * q.dt)
+            target.append(vz_row(u).clone())
+
+    def loss_fn(u, n):
+        return ((vz_row(u) - target[n - 1]) ** 2).sum()
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        out = fn()
+        b.record()
+        torch.cuda.synchronize()
+        return out, a.elapsed_time(b)
+
+    for _ in range(max(args.warmup, 1)):
+        with torch.no_grad():
+            rollout(sa, theta0, u0, 20, loss_fn, checkpoint_every=20)
+    with torch.no_grad():
+        L0, ms_fwd = timed(lambda: rollout(sa, theta0, u0, nsteps, loss_fn, checkpoint_every=20))
+
+    def fwd_bwd():
+        th = theta0.clone().requires_grad_(True)
+        L = rollout(sa, th, u0, nsteps, loss_fn, checkpoint_every=20)
+        L.backward()
+        return th.grad.clone()
+
+    grad, ms_fb = timed(fwd_bwd)
+    fd = []
+    for k in range(3):
+        h = 1e-4 * float(theta0[k])
+        vals = []
+        for sgn in (1, -1):
+            th = theta0.clone()
+            th[k] += sgn * h
+            with torch.no_grad():
+                vals.append(float(rollout(sa, th, u0, nsteps, loss_fn, checkpoint_every=20)))
+        fd.append((vals[0] - vals[1]) / (2 * h))
+    rel = [abs(float(grad[k]) - fd[k]) / max(abs(fd[k]), 1e-300) for k in range(3)]
+    sa.close()
+    cells = p.interior_cells()
+    line = {
+        "metric": "adjoint cost / forward cost (loss gradient over a 400-step RK4 rollout)",
+        "value": ms_fb / ms_fwd, "unit": "x forward", "n_gpus": 1, "steps": nsteps, "warmup": args.warmup,
+        "ms_per_step": ms_fb / nsteps, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "2D stratified slab 256x512, driver gradient, dt fixed, "
+                               "checkpoints every 20 steps", "interior_cells": cells,
+                   "observed_row_z_m": float(pos[0][0][kz]), "dt_s": q.dt},
+        "forward_ms": ms_fwd, "forward_backward_ms": ms_fb,
+        "forward_mcell_updates_per_s": cells * nsteps / (ms_fwd / 1e3) / 1e6,
+        "loss": float(L0), "grad": [float(g) for g in grad], "fd": fd, "fd_rel_err": rel,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def dist_setup(args):
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -350,7 +460,10 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="ot", choices=["ot", "tube", "ensemble"])
+    ap.add_argument("--workload", default="ot", choices=["ot", "tube", "ensemble", "adjoint"])
+    ap.add_argument("--adj-steps", type=int, default=400)
+    ap.add_argument("--obs-z", type=float, default=3.0e6,
+                    help="height of the observed v_z row for --workload adjoint [m]")
     ap.add_argument("--nruns", type=int, default=64)
     ap.add_argument("--precision", default=None, choices=["fp64", "mixed"],
                     help="default: fp64 (ot, tube; mixed reported beside it), mixed (ensemble)")
@@ -372,6 +485,9 @@ def main():
         args.precision = "mixed" if args.workload == "ensemble" else "fp64"
     if args.workload == "ensemble" and args.impl != "reference":
         ensemble_main(args)
+        return
+    if args.workload == "adjoint" and args.impl != "reference":
+        adjoint_main(args)
         return
     if args.impl == "reference":
         reference_arm(args, ws, rank)
