@@ -56,6 +56,12 @@ METRIC = "Mcell-updates/s per RK4 step"
 UNIT = "Mcell-updates/s"
 
 
+# DRAM bytes per interior cell per RK4 step measured by ncu on all four stage
+# launches (profiles/dram_traffic_per_stage.md: 2D at 2048^2, 3D at 128^3)
+TRAFFIC_PER_CELL_STEP = {(2, "fp64"): 865.8, (2, "mixed"): 723.8, (3, "fp64"): 1482.3,
+                         (3, "mixed"): 1230.8}
+
+
 def alg_bytes_mixed(ndim):
     """The same for the mixed form: stage states in float (4 B), the base
     state as a float high/low pair (8 B), accumulator and backgrounds in
@@ -612,7 +618,8 @@ def main():
                  "rel_l2_vs_fp64": {"steps": args.warmup + args.steps, "max": max(errs),
                                     "per_field": errs},
                  "roofline": {"bound": "hbm", "achieved": mach, "peak": peak_m, "unit": "GB/s",
-                              "frac": mach / peak_m, "alg_bytes_per_cell_step": mbytes}}
+                              "frac": mach / peak_m, "alg_bytes_per_cell_step": mbytes,
+                              "traffic": TRAFFIC_PER_CELL_STEP[(p.ndim, "mixed")] * ncell_int / 4}}
 
     if rank == 0:
         peak, pk_kind = peaks()
@@ -633,7 +640,10 @@ def main():
                     "gpu_launches_per_step": 4 + 2},
             "gpu_launches": launches,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None,
+                         "frac": achieved / peak,
+                         "traffic": TRAFFIC_PER_CELL_STEP.get((p.ndim, args.precision), 0.0)
+                         * ncell_int / 4 or None,
+                         "traffic_unit": "bytes per stage launch (ncu, scaled by cells)",
                          "peak_kind": pk_kind,
                          "alg_bytes_per_cell_step": alg_bytes,
                          "note": "stage kernel; FP64 arithmetic, not HBM, limits this form"},
