@@ -433,11 +433,15 @@ def reference_arm(args, ws, rank):
     print(json.dumps(line), flush=True)
 
 
-def reference_gpu_binary(timeout=240):
+def reference_gpu_binary(timeout=240, name="ot1024t",
+                         kind="reference binary built from source, its own per-step timer"):
     """Per-step time of the reference's own GPU binary (built from its
     sources by oracle/build_ref.py, Euler, 1024^2): Mcell-updates/s per
-    Euler step from its own 'time total' lines, first 5 steps discarded."""
-    binp = os.path.join(ROOT, "oracle", "_ref", "ot1024t", "smaug")
+    Euler step from its own 'time total' lines, first 5 steps discarded.
+    name="compat_ot1024t" times the same unchanged driver linked against the
+    wrapper shim (libsmaug_compat2d.so), i.e. the reference's host loop
+    driving this engine."""
+    binp = os.path.join(ROOT, "oracle", "_ref", name, "smaug")
     if not os.path.exists(binp):
         return None
     import tempfile
@@ -457,7 +461,7 @@ def reference_gpu_binary(timeout=240):
     per = (tt[-1] - tt[4]) / (len(tt) - 5)
     return {"value": 1024 * 1024 / per / 1e6, "unit": "Mcell-updates/s per Euler step",
             "ms_per_step": per * 1e3, "workload": "2D Orszag-Tang 1024x1024, FP64, Euler",
-            "kind": "reference binary built from source, its own per-step timer"}
+            "kind": kind}
 
 
 def main():
@@ -659,6 +663,10 @@ def main():
                                                   args.ref_sample, args.ref_sample, el)}
         if ws == 1 and not args.no_ref_gpu and args.workload == "ot":
             line["reference_gpu"] = reference_gpu_binary()
+            line["reference_driver_on_engine"] = reference_gpu_binary(
+                name="compat_ot1024t",
+                kind="the reference's unchanged driver (src/iosmaug.c) linked against "
+                     "libsmaug_compat2d.so, its own per-step timer")
         print(json.dumps(line), flush=True)
     if ws > 1:
         import torch.distributed as dist

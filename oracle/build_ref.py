@@ -77,52 +77,81 @@ def _set_define(text, name, value):
     return pat.sub("#define %s %s" % (name, value), text)
 
 
+def _configure(tmp, ni, nj, nt, nk, cfg):
+    """Copy the reference tree to tmp and select the model and run parameters
+    as `make ot` / `make fluxtube1` does; returns (src, inc)."""
+    three = nk is not None
+    for d in ("src", "include", "models"):
+        shutil.copytree(os.path.join(REFROOT, d), os.path.join(tmp, d))
+    subprocess.check_call(["chmod", "-R", "u+w", tmp])
+    src, inc, mod = (os.path.join(tmp, d) for d in ("src", "include", "models"))
+    model = "fluxtube1" if three else "ot"
+    # make ot / make fluxtube1 (src/Makefile:32-101)
+    shutil.copy(os.path.join(mod, "iosmaugparams.h." + model), os.path.join(inc, "iosmaugparams.h"))
+    shutil.copy(os.path.join(mod, "init_user.cu." + model), os.path.join(src, "init_user.cu"))
+    shutil.copy(os.path.join(mod, "boundary.cu." + model), os.path.join(src, "boundary.cu"))
+    if three:
+        shutil.copy(os.path.join(mod, "usersource.cu." + model), os.path.join(src, "usersource.cu"))
+        shutil.copy(os.path.join(mod, "initialisation_user.h.default"),
+                    os.path.join(inc, "initialisation_user.h"))
+    ph = os.path.join(inc, "iosmaugparams.h")
+    text = open(ph).read()
+    text = _set_define(text, "NI", str(ni))
+    text = _set_define(text, "NJ", str(nj))
+    text = _set_define(text, "NT", str(nt))
+    keys = ["XMIN", "XMAX", "YMIN", "YMAX", "DT", "PCOURANT", "PMODDTON",
+            "PCFGSAVEFREQUENCY", "PGAMMA", "CFGFILE", "CFGOUT"]
+    if three:
+        text = _set_define(text, "NK", str(nk))
+        keys += ["ZMIN", "ZMAX", "PGRAV0", "PGRAV1", "PGRAV2"]
+    for k in keys:
+        text = _set_define(text, k, cfg[k])
+    for k in ("PCHYP", "PCHYPRHO", "PCHYPENERGY", "PCHYPB0", "PCHYPB1", "PCHYPB2",
+              "PCHYPMOM0", "PCHYPMOM1", "PCHYPMOM2"):
+        text = _set_define(text, k, cfg.get(k, cfg["CHYP"]))
+    open(ph, "w").write(text)
+    return src, inc
+
+
+def _driver_objects(src, three, verbose):
+    """The reference's host driver (g++, as src/make_inputs:3 selects)."""
+    sac = "-DUSE_SAC_3D" if three else "-DUSE_SAC"
+    objs = []
+    for c in (CFILES_3D if three else CFILES):
+        o = os.path.join(src, c.rsplit(".", 1)[0] + ".o")
+        cmd = ["g++", "-O0", "-fno-unreachable-traps", sac, "-DD1D", "-w", "-fpermissive",
+               "-o", o, "-c", os.path.join(src, c)]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.check_call(cmd, cwd=src)
+        objs.append(o)
+    return objs
+
+
+def _cached(name, stamp):
+    dest = os.path.join(OUT, name)
+    os.makedirs(dest, exist_ok=True)
+    binp = os.path.join(dest, "smaug")
+    stampf = os.path.join(dest, "build.txt")
+    fresh = os.path.exists(binp) and os.path.exists(stampf) and open(stampf).read() == stamp
+    return binp, stampf, fresh
+
+
 def build_ref(name, ni, nj, nt, arch="sm_100a", verbose=True, nk=None, **kw):
     if not os.path.isdir(REFROOT):
         raise RuntimeError("reference sources not present at %s" % REFROOT)
     cfg = dict(DEFAULTS)
     cfg.update({k.upper(): str(v) for k, v in kw.items()})
-    dest = os.path.join(OUT, name)
-    os.makedirs(dest, exist_ok=True)
     three = nk is not None
     if three and nk > nj:
         raise ValueError("3D reference builds need nk <= nj")
     stamp = "ni=%d nj=%d nk=%s nt=%d %s arch=%s\n" % (ni, nj, nk, nt, sorted(cfg.items()), arch)
-    binp = os.path.join(dest, "smaug")
-    stampf = os.path.join(dest, "build.txt")
-    if os.path.exists(binp) and os.path.exists(stampf) and open(stampf).read() == stamp:
+    binp, stampf, fresh = _cached(name, stamp)
+    if fresh:
         return binp
     tmp = tempfile.mkdtemp(prefix="smaug_ref_")
     try:
-        for d in ("src", "include", "models"):
-            shutil.copytree(os.path.join(REFROOT, d), os.path.join(tmp, d))
-        subprocess.check_call(["chmod", "-R", "u+w", tmp])
-        src, inc, mod = (os.path.join(tmp, d) for d in ("src", "include", "models"))
-        model = "fluxtube1" if three else "ot"
-        # make ot / make fluxtube1 (src/Makefile:32-101)
-        shutil.copy(os.path.join(mod, "iosmaugparams.h." + model), os.path.join(inc, "iosmaugparams.h"))
-        shutil.copy(os.path.join(mod, "init_user.cu." + model), os.path.join(src, "init_user.cu"))
-        shutil.copy(os.path.join(mod, "boundary.cu." + model), os.path.join(src, "boundary.cu"))
-        if three:
-            shutil.copy(os.path.join(mod, "usersource.cu." + model), os.path.join(src, "usersource.cu"))
-            shutil.copy(os.path.join(mod, "initialisation_user.h.default"),
-                        os.path.join(inc, "initialisation_user.h"))
-        ph = os.path.join(inc, "iosmaugparams.h")
-        text = open(ph).read()
-        text = _set_define(text, "NI", str(ni))
-        text = _set_define(text, "NJ", str(nj))
-        text = _set_define(text, "NT", str(nt))
-        keys = ["XMIN", "XMAX", "YMIN", "YMAX", "DT", "PCOURANT", "PMODDTON",
-                "PCFGSAVEFREQUENCY", "PGAMMA", "CFGFILE", "CFGOUT"]
-        if three:
-            text = _set_define(text, "NK", str(nk))
-            keys += ["ZMIN", "ZMAX", "PGRAV0", "PGRAV1", "PGRAV2"]
-        for k in keys:
-            text = _set_define(text, k, cfg[k])
-        for k in ("PCHYP", "PCHYPRHO", "PCHYPENERGY", "PCHYPB0", "PCHYPB1", "PCHYPB2",
-                  "PCHYPMOM0", "PCHYPMOM1", "PCHYPMOM2"):
-            text = _set_define(text, k, cfg.get(k, cfg["CHYP"]))
-        open(ph, "w").write(text)
+        src, inc = _configure(tmp, ni, nj, nt, nk, cfg)
         # workaround 1 (see module docstring)
         initcu = os.path.join(src, "init.cu")
         lines = open(initcu).read().split("\n")
@@ -147,15 +176,47 @@ def build_ref(name, ni, nj, nt, arch="sm_100a", verbose=True, nk=None, **kw):
                 print(" ".join(cmd), flush=True)
             subprocess.check_call(cmd, cwd=src)
             objs.append(o)
-        for c in (CFILES_3D if three else CFILES):
-            o = os.path.join(src, c.rsplit(".", 1)[0] + ".o")
-            cmd = ["g++", "-O0", "-fno-unreachable-traps", sac, "-DD1D", "-w", "-fpermissive",
-                   "-o", o, "-c", os.path.join(src, c)]
-            if verbose:
-                print(" ".join(cmd), flush=True)
-            subprocess.check_call(cmd, cwd=src)
-            objs.append(o)
+        objs += _driver_objects(src, three, verbose)
         cmd = ["nvcc", "-arch=" + arch, "-o", binp] + objs + ["-lcudart", "-lm"]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.check_call(cmd, cwd=src)
+        with open(stampf, "w") as f:
+            f.write(stamp)
+        return binp
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+
+
+def build_compat(name, ni, nj, nt, verbose=True, nk=None, **kw):
+    """The reference's unchanged host driver (src/iosmaug.c, readwrite.c,
+    initialisation.c, dxroutines.c) linked against this project's wrapper
+    shim smaug_b200/libsmaug_compat{2d,3d}.so instead of the reference's .cu
+    objects.  Same parameters as build_ref; the binary finds the shim through
+    an rpath relative to its own location (oracle/_ref/<name>/smaug)."""
+    if not os.path.isdir(REFROOT):
+        raise RuntimeError("reference sources not present at %s" % REFROOT)
+    cfg = dict(DEFAULTS)
+    cfg.update({k.upper(): str(v) for k, v in kw.items()})
+    three = nk is not None
+    if three and nk > nj:
+        raise ValueError("3D reference builds need nk <= nj")
+    pkg = os.path.join(os.path.dirname(HERE), "smaug_b200")
+    shim = os.path.join(pkg, "libsmaug_compat%s.so" % ("3d" if three else "2d"))
+    if not os.path.exists(shim):
+        raise RuntimeError("build the package first (smaug_b200/build.py): %s missing" % shim)
+    stamp = "compat ni=%d nj=%d nk=%s nt=%d %s shim=%s\n" % (ni, nj, nk, nt, sorted(cfg.items()),
+                                                          os.path.getmtime(shim))
+    binp, stampf, fresh = _cached(name, stamp)
+    if fresh:
+        return binp
+    tmp = tempfile.mkdtemp(prefix="smaug_compat_")
+    try:
+        src, inc = _configure(tmp, ni, nj, nt, nk, cfg)
+        objs = _driver_objects(src, three, verbose)
+        cmd = ["g++", "-o", binp] + objs + [
+            "-L", pkg, "-lsmaug_compat%s" % ("3d" if three else "2d"), "-lsmaug_b200",
+            "-Wl,-rpath,$ORIGIN/../../../smaug_b200", "-lm"]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.check_call(cmd, cwd=src)
@@ -176,10 +237,25 @@ STANDARD = [
 ]
 
 
+_T3 = {"XMIN": "0.0", "XMAX": "0.1", "YMIN": "0.0", "YMAX": "0.1", "ZMIN": "0.0",
+       "ZMAX": "0.1", "PGRAV0": "-0.1", "PGRAV1": "0.0", "PGRAV2": "0.0"}
+# The same driver builds linked against the wrapper shim (tests/test_compat.py
+# runs them on the golden fixtures' inputs; the 1024^2 one times the unchanged
+# driver on the engine beside ot1024t).
+COMPAT_STANDARD = [
+    ("compat_g16", 16, 16, 21, None, {}),
+    ("compat_g18x12", 18, 12, 21, None, {}),
+    ("compat_t3s", 4, 4, 21, 4, _T3),
+    ("compat_ot1024t", 1024, 1024, 12, None, {"PCFGSAVEFREQUENCY": "100000"}),
+]
+
+
 def build_standard(verbose=False):
     out = {}
     for name, ni, nj, nt, kw in STANDARD:
         out[name] = build_ref(name, ni, nj, nt, verbose=verbose, **kw)
+    for name, ni, nj, nt, nk, kw in COMPAT_STANDARD:
+        out[name] = build_compat(name, ni, nj, nt, verbose=verbose, nk=nk, **kw)
     return out
 
 

@@ -1,4 +1,6 @@
-"""Build the engine shared library (sm_100a) in-tree: smaug_b200/libsmaug_b200.so.
+"""Build the engine shared library (sm_100a) in-tree: smaug_b200/libsmaug_b200.so,
+and the reference-wrapper shims libsmaug_compat2d.so / libsmaug_compat3d.so on
+top of it (host C++, one per NDIM as the reference's struct params differs).
 
 The translation units (the 2D and 3D stage kernels, the engine host code and
 the file formats) compile to objects in parallel under smaug_b200/_build/,
@@ -19,6 +21,11 @@ SRCS = [os.path.join(CSRC, f) for f in ("engine.cu", "stage2d.cu", "stage3d.cu",
                                          "adjoint.cu", "host_io.cpp")]
 HEADERS = [os.path.join(CSRC, f) for f in sorted(os.listdir(CSRC)) if f.endswith((".h", ".cuh"))] + [
     os.path.join(ROOT, "include", "smaug_b200.h")]
+COMPAT_SRC = os.path.join(CSRC, "compat.cpp")
+COMPAT_HDR = os.path.join(ROOT, "include", "smaug_compat.h")
+# (library, build macro of the reference): USE_SAC = 2D, USE_SAC_3D = 3D
+COMPAT = [(os.path.join(HERE, "libsmaug_compat2d.so"), "-DUSE_SAC"),
+          (os.path.join(HERE, "libsmaug_compat3d.so"), "-DUSE_SAC_3D")]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2"]
 
@@ -54,6 +61,15 @@ def build(force=False, verbose=False, extra=()):
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.check_call(cmd)
+    for lib, macro in COMPAT:
+        if force or _stale(lib, [COMPAT_SRC, COMPAT_HDR, os.path.join(ROOT, "include", "smaug_b200.h"),
+                                 LIB]):
+            cmd = ["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-Wall", macro,
+                   "-I", os.path.join(ROOT, "include"), "-o", lib, COMPAT_SRC,
+                   "-L", HERE, "-lsmaug_b200", "-Wl,-rpath,$ORIGIN"]
+            if verbose:
+                print(" ".join(cmd), flush=True)
+            subprocess.check_call(cmd)
     return LIB
 
 
