@@ -40,8 +40,11 @@
  *                        (src/update.cu:207) does
  * Unsupported: rkon=1 (the reference's RK driver), divbon=1, shock viscosity,
  * fields of one dimension with different boundary types, boundary types
- * other than periodic (0) and contcd4 (4) (also for the init-time fixed
- * boundary sweep).  The reference's wrappers report no errors and the driver
+ * other than periodic (0), contcd4 (4) and fixed (5: the ghost layers keep
+ * their initial values, as in the OT model build, whose cuboundary dispatches
+ * periodic only, src/boundary.cu:231-252); cont, symm and asymm are left out
+ * because no model's cuboundary dispatches them, so their meaning depends on
+ * the model file.  The reference's wrappers report no errors and the driver
  * ignores their return values, so an unsupported use or an engine error is
  * printed to stderr and ends the process with status 3.
  *

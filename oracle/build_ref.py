@@ -106,6 +106,10 @@ def _configure(tmp, ni, nj, nt, nk, cfg):
         keys += ["ZMIN", "ZMAX", "PGRAV0", "PGRAV1", "PGRAV2"]
     for k in keys:
         text = _set_define(text, k, cfg[k])
+    # boundary types per dimension (BCU*: upper, BCL*: lower), when given
+    for k in ("BCU0", "BCL0", "BCU1", "BCL1") + (("BCU2", "BCL2") if three else ()):
+        if k in cfg:
+            text = _set_define(text, k, cfg[k])
     for k in ("PCHYP", "PCHYPRHO", "PCHYPENERGY", "PCHYPB0", "PCHYPB1", "PCHYPB2",
               "PCHYPMOM0", "PCHYPMOM1", "PCHYPMOM2"):
         text = _set_define(text, k, cfg.get(k, cfg["CHYP"]))

@@ -1016,8 +1016,14 @@ static void k_source(O *o) {
 /* ---- ghost cells -------------------------------------------------------- */
 /* periodic: boundary0/1_parallel (src/boundary.cu:72-225), bc3_periodic1_dir
    (src/gradops.cu:1270-1320); contcd4: models/boundary.cu.fluxtube1:16-85;
-   cont/symm/asymm: src/gradops.cu:947-1060,1325-1465.  Applied per field
-   (rho..b_last) and per dim in the reference's order (src/iosmaug.c:830-833). */
+   cont/symm/asymm: src/gradops.cu:947-1060,1325-1465 (symm/asymm mirror about
+   the face between cells 1 and 2 in 2D, about cell 2 in the 3D branch);
+   fixed: the ghost cells are not written (the OT model's cuboundary,
+   src/boundary.cu:231-252, dispatches periodic only, and the flux-tube model
+   restores type 5 from a store its init sweep never fills,
+   models/boundary.cu.fluxtube1:1137-1277), so they keep their initial values.
+   Applied per field (rho..b_last) and per dim in the reference's order
+   (src/iosmaug.c:830-833). */
 static void bc_field_dir(const O *o, double *w, int f, int dir) {
   int n = o->n[dir];
   int type = o->P->boundtype[dir][0];
@@ -1045,9 +1051,16 @@ static void bc_field_dir(const O *o, double *w, int f, int dir) {
         break;
       case SMAUG_BC_SYMM:
       case SMAUG_BC_ASYMM:
-        if (x == 0 || x == 1) src = 3 - x;
-        else if (x == n - 1 || x == n - 2) src = 2 * n - 5 - x;
+        if (o->nd == 3) {
+          if (x == 0 || x == 1) src = 4 - x;
+          else if (x == n - 1 || x == n - 2) src = 2 * n - 6 - x;
+        } else {
+          if (x == 0 || x == 1) src = 3 - x;
+          else if (x == n - 1 || x == n - 2) src = 2 * n - 5 - x;
+        }
         if (type == SMAUG_BC_ASYMM) sgn = -1.0;
+        break;
+      case SMAUG_BC_FIXED:
         break;
       default:
         break;

@@ -906,9 +906,8 @@ static int adj_create(const smaug_params_t* p, const double* w, const double* po
   K.n1 = n1;
   K.n2 = 1;
   K.ncell = nc;
+  set_boundaries(K, p, 2);
   for (int d = 0; d < 3; d++) {
-    K.bt[d] = d < 2 ? p->boundtype[d][0] : 0;
-    K.bc[d] = K.bt[d];
     K.dx[d] = p->dx[d];
     K.g[d] = p->g[d];
     K.drv_x0[d] = p->drv_x0[d];

@@ -189,11 +189,13 @@ int initgrid(params** p, state**, double** wd, params**, double**, double**, sta
 int cuboundary(params** p, bparams**, params**, bparams**, state**, double**, int, int idir,
                int field) {
   need_started("cuboundary");
-  int t0 = (*p)->boundtype[field][idir][0], t1 = (*p)->boundtype[field][idir][1];
-  if (t0 != SMAUG_BC_PERIODIC && t0 != SMAUG_BC_CONTCD4)
-    die("cuboundary", "boundary type other than periodic (0) or contcd4 (4)");
-  if (t1 != SMAUG_BC_PERIODIC && t1 != SMAUG_BC_CONTCD4)
-    die("cuboundary", "boundary type other than periodic (0) or contcd4 (4)");
+  // types whose meaning does not depend on the model's boundary.cu: periodic,
+  // contcd4 and fixed (ghosts keep their initial values)
+  for (int side = 0; side < 2; side++) {
+    const int t = (*p)->boundtype[field][idir][side];
+    if (t != SMAUG_BC_PERIODIC && t != SMAUG_BC_CONTCD4 && t != SMAUG_BC_FIXED)
+      die("cuboundary", "boundary type other than periodic (0), contcd4 (4) or fixed (5)");
+  }
   return 0;  // the engine's step writes the ghost layers
 }
 

@@ -73,7 +73,8 @@ __global__ void ghost_fill2d_kernel(const KParams P, double* u) {
   int sj = ghost_source(j, P.n1, P.bc[1]);
   if (si == i && sj == j) return;
   long s = (long)sj * P.n0 + si;
-  for (int f = 0; f < 6; f++) u[f * P.ncell + c] = u[f * P.ncell + s];
+  const bool neg = ((si != i) && P.gneg[0]) != ((sj != j) && P.gneg[1]);
+  for (int f = 0; f < 6; f++) u[f * P.ncell + c] = neg ? -u[f * P.ncell + s] : u[f * P.ncell + s];
 }
 
 __global__ void ghost_fill3d_kernel(const KParams P, double* u) {
@@ -85,14 +86,26 @@ __global__ void ghost_fill3d_kernel(const KParams P, double* u) {
   int sk = ghost_source(k, P.n2, P.bc[2]);
   if (si == i && sj == j && sk == k) return;
   long s = ((long)sk * P.n1 + sj) * P.n0 + si;
-  for (int f = 0; f < 8; f++) u[f * P.ncell + c] = u[f * P.ncell + s];
+  const bool neg = (((si != i) && P.gneg[0]) != ((sj != j) && P.gneg[1])) != ((sk != k) && P.gneg[2]);
+  for (int f = 0; f < 8; f++) u[f * P.ncell + c] = neg ? -u[f * P.ncell + s] : u[f * P.ncell + s];
+}
+
+// cells that the stage kernels never write: a ghost coordinate along a dim
+// with fixed boundaries
+__device__ __forceinline__ bool fixed_ghost(const KParams& P, int i, int j, int k) {
+  return (P.bc[0] == SMAUG_BC_FIXED && (i < 2 || i > P.n0 - 3)) ||
+         (P.bc[1] == SMAUG_BC_FIXED && (j < 2 || j > P.n1 - 3)) ||
+         (P.n2 > 1 && P.bc[2] == SMAUG_BC_FIXED && (k < 2 || k > P.n2 - 3));
 }
 
 __global__ void cmax3d_kernel(const KParams P, const double* u, const double* bg,
-                              unsigned long long* out) {
+                              unsigned long long* out, int fixed_only) {
   long c = blockIdx.x * (long)blockDim.x + threadIdx.x;
   double cm[3] = {0, 0, 0};
-  if (c < P.ncell) {
+  bool use = c < P.ncell;
+  if (use && fixed_only)
+    use = fixed_ghost(P, (int)(c % P.n0), (int)((c / P.n0) % P.n1), (int)(c / ((long)P.n0 * P.n1)));
+  if (use) {
     const long nc = P.ncell;
     double s[8], g[5];
     for (int f = 0; f < 8; f++) s[f] = u[f * nc + c];
@@ -108,10 +121,12 @@ __global__ void cmax3d_kernel(const KParams P, const double* u, const double* bg
 }
 
 __global__ void cmax2d_kernel(const KParams P, const double* u, const double* bg,
-                              unsigned long long* out) {
+                              unsigned long long* out, int fixed_only) {
   long c = blockIdx.x * (long)blockDim.x + threadIdx.x;
   double cm[2] = {0, 0};
-  if (c < P.ncell) {
+  bool use = c < P.ncell;
+  if (use && fixed_only) use = fixed_ghost(P, (int)(c % P.n0), (int)(c / P.n0), 0);
+  if (use) {
     const long nc = P.ncell;
     for (int d = 0; d < 2; d++)
       cm[d] = cfast2(P.gamma, u[0 * nc + c], u[1 * nc + c], u[2 * nc + c], u[3 * nc + c],
@@ -202,8 +217,13 @@ static int validate(const smaug_params_t* p) {
     int b = p->boundtype[d][0];
     if (b != p->boundtype[d][1])
       return set_error(SMAUG_E_UNSUPPORTED, "dim %d: different upper/lower boundary types", d);
-    if (b != SMAUG_BC_PERIODIC && b != SMAUG_BC_CONTCD4 && b != SMAUG_BC_CONT && b != SMAUG_BC_SYMM)
+    if (b != SMAUG_BC_PERIODIC && b != SMAUG_BC_CONTCD4 && b != SMAUG_BC_CONT && b != SMAUG_BC_SYMM &&
+        b != SMAUG_BC_ASYMM && b != SMAUG_BC_FIXED)
       return set_error(SMAUG_E_UNSUPPORTED, "dim %d: boundary type %d not supported", d, b);
+    // the reference adds the driver term to every cell, ghosts included
+    // (src/centdiff2.cu:790-872); only fixed ghost cells would keep it
+    if (b == SMAUG_BC_FIXED && p->driver != SMAUG_DRIVER_NONE)
+      return set_error(SMAUG_E_UNSUPPORTED, "dim %d: fixed boundaries with a driver term", d);
   }
   if (p->moddton == 1 && !(p->courant > 0))
     return set_error(SMAUG_E_INVALID, "courant must be > 0 with moddton");
@@ -308,9 +328,8 @@ static int create(const smaug_params_t* p, const double* w, const double* pos, E
   K.n1 = p->n[1];
   K.n2 = n2;
   K.ncell = nc;
+  set_boundaries(K, p, e->nd);
   for (int d = 0; d < 3; d++) {
-    K.bt[d] = (d < e->nd) ? p->boundtype[d][0] : 0;
-    K.bc[d] = (d < e->nd) ? p->boundtype[d][0] : 0;
     K.dx[d] = p->dx[d];
     K.g[d] = p->g[d];
     K.drv_x0[d] = p->drv_x0[d];
@@ -328,6 +347,17 @@ static int create(const smaug_params_t* p, const double* w, const double* pos, E
   for (int f = 2 + 2 * e->nd; f < nvar && !K.has_bg; f++)
     for (long c = 0; c < nc; c++)
       if (w[(size_t)f * nc + c] != 0.0) { K.has_bg = 1; break; }
+  // The reference's 2D gravity (src/centdiff2.cu:721-787) and background
+  // energy coupling (src/centdiff2.cu:587-717) also update ghost cells; with
+  // fixed boundaries nothing overwrites them there, so those ghost layers
+  // drift.  The engine keeps fixed ghost cells constant, which agrees with
+  // the reference only without both terms.  (Its 3D kernels stay interior.)
+  if (e->nd == 2 && has_fixed(K) && (K.has_bg || K.has_grav)) {
+    delete e;
+    return set_error(SMAUG_E_UNSUPPORTED,
+                     "2D fixed boundaries with gravity or background fields: the reference also "
+                     "updates those ghost layers");
+  }
   K.driver = p->driver;
   K.drv_amp = p->drv_amp;
   K.drv_period = p->drv_period;
@@ -364,7 +394,7 @@ static int create(const smaug_params_t* p, const double* w, const double* pos, E
     E_TRY(cudaMalloc(&e->d_pad[d], sizeof(int) * ps.size()));
     E_TRY(cudaMemcpy(e->d_pad[d], ps.data(), sizeof(int) * ps.size(), cudaMemcpyHostToDevice));
   }
-  E_TRY(cudaMalloc(&e->d_cmax, sizeof(unsigned long long) * 9));
+  E_TRY(cudaMalloc(&e->d_cmax, sizeof(unsigned long long) * 12));  // ring of 3 + fixed floor
   E_TRY(cudaMalloc(&e->d_dt, sizeof(double) * 2));
   E_TRY(cudaMalloc(&e->d_t, sizeof(double) * 2));
   E_TRY(cudaMalloc(&e->d_flags, sizeof(int)));
@@ -429,14 +459,42 @@ static int reset_derived(Engine* e) {
   CUDA_TRY(cudaMemsetAsync(e->d_cmax, 0, sizeof(unsigned long long) * 9, e->stream));
   unsigned long long* slot = e->d_cmax + 3 * (e->stage_count % 3);
   if (e->nd == 3)
-    cmax3d_kernel<<<(unsigned)nb, bs, 0, e->stream>>>(e->K, u, e->d_bg, slot);
+    cmax3d_kernel<<<(unsigned)nb, bs, 0, e->stream>>>(e->K, u, e->d_bg, slot, 0);
   else
-    cmax2d_kernel<<<(unsigned)nb, bs, 0, e->stream>>>(e->K, u, e->d_bg, slot);
+    cmax2d_kernel<<<(unsigned)nb, bs, 0, e->stream>>>(e->K, u, e->d_bg, slot, 0);
   CUDA_TRY(cudaGetLastError());
+  const long n = (long)e->nevo * e->ncell;
   if (e->mix) {
-    const long n = (long)e->nevo * e->ncell;
     split_kernel<<<(unsigned)((n + bs - 1) / bs), bs, 0, e->stream>>>(u, base_hi(e), base_lo(e), n);
     CUDA_TRY(cudaGetLastError());
+  }
+  if (has_fixed(e->K)) {
+    // fixed ghost cells are written by no stage: every buffer gets them now,
+    // and their CFL maxima become the floor of every later maximum
+    if (!e->mix) {
+      for (int i = 0; i < 3; i++)
+        if (e->d_u[i] && e->d_u[i] != u)
+          CUDA_TRY(cudaMemcpyAsync(e->d_u[i], u, sizeof(double) * n, cudaMemcpyDeviceToDevice, e->stream));
+    } else {
+      const int other = 1 - e->cur;
+      split_kernel<<<(unsigned)((n + bs - 1) / bs), bs, 0, e->stream>>>(u, e->d_h[2 * other],
+                                                                          e->d_h[2 * other + 1], n);
+      CUDA_TRY(cudaGetLastError());
+      if (e->P.integrator == SMAUG_INT_RK4)  // h2, h3 are plain stage buffers
+        CUDA_TRY(cudaMemcpyAsync(e->d_h[3], e->d_h[2], sizeof(float) * n, cudaMemcpyDeviceToDevice,
+                                 e->stream));
+    }
+    unsigned long long* fl = e->d_cmax + 9;
+    CUDA_TRY(cudaMemsetAsync(fl, 0, sizeof(unsigned long long) * 3, e->stream));
+    if (e->nd == 3)
+      cmax3d_kernel<<<(unsigned)nb, bs, 0, e->stream>>>(e->K, u, e->d_bg, fl, 1);
+    else
+      cmax2d_kernel<<<(unsigned)nb, bs, 0, e->stream>>>(e->K, u, e->d_bg, fl, 1);
+    CUDA_TRY(cudaGetLastError());
+    double floor3[3] = {0, 0, 0};
+    CUDA_TRY(cudaMemcpyAsync(floor3, fl, sizeof(floor3), cudaMemcpyDeviceToHost, e->stream));
+    CUDA_TRY(cudaStreamSynchronize(e->stream));
+    for (int d = 0; d < 3; d++) e->K.cmax_floor[d] = d < e->nd ? floor3[d] : 0.0;
   }
   return SMAUG_OK;
 }
@@ -1101,6 +1159,8 @@ extern "C" int smaug_euler_step_noalloc(const smaug_params_t* p, const double* w
                      p->n[0], p->n[1], NOALLOC_MAXN);
   if (p->driver != SMAUG_DRIVER_NONE)
     return set_error(SMAUG_E_UNSUPPORTED, "the allocation-free step has no driver term");
+  if (p->boundtype[0][0] == SMAUG_BC_FIXED || p->boundtype[1][0] == SMAUG_BC_FIXED)
+    return set_error(SMAUG_E_UNSUPPORTED, "the allocation-free step has no fixed boundaries");
   unsigned char* s = nullptr;
   if ((rc = noalloc_scratch(&s))) return rc;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
@@ -1111,9 +1171,8 @@ extern "C" int smaug_euler_step_noalloc(const smaug_params_t* p, const double* w
   K.n1 = p->n[1];
   K.n2 = 1;
   K.ncell = nc;
+  set_boundaries(K, p, 2);
   for (int d = 0; d < 3; d++) {
-    K.bt[d] = (d < 2) ? p->boundtype[d][0] : 0;
-    K.bc[d] = K.bt[d];
     K.dx[d] = p->dx[d];
     K.g[d] = p->g[d];
   }
@@ -1144,7 +1203,7 @@ extern "C" int smaug_euler_step_noalloc(const smaug_params_t* p, const double* w
                                                          pad + NOALLOC_MAXN);
   CUDA_TRY(cudaGetLastError());
   const double* bg = w_in + 6 * nc;
-  cmax2d_kernel<<<(unsigned)((nc + 255) / 256), 256, 0, st>>>(K, w_in, bg, cm);
+  cmax2d_kernel<<<(unsigned)((nc + 255) / 256), 256, 0, st>>>(K, w_in, bg, cm, 0);
   CUDA_TRY(cudaGetLastError());
   KBufs B{};
   B.uin = w_in;

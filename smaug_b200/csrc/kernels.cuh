@@ -40,7 +40,9 @@ struct KParams {
   int n0, n1, n2;   // n2 = 1 in 2D
   long ncell;
   int bt[3];        // boundtype[dim][0] (upper) -- gradient edge zeroing
-  int bc[3];        // ghost-fill type per dim
+  int bc[3];        // ghost-fill type per dim (image pattern; FIXED: no images)
+  int gneg[3];      // 1: ghost images along dim are negated (antisymmetric)
+  double cmax_floor[3];  // CFL maxima over the fixed ghost cells (constant in time)
   double gamma, courant, dtmax;
   double dx[3];
   double g[3];
@@ -48,6 +50,26 @@ struct KParams {
   int moddton, hyperdif, has_bg, has_grav, driver;
   double drv_amp, drv_period, drv_x0[3], drv_sigma[3];
 };
+
+// Boundary fields of KParams from the per-dimension types of p.  Ghost images
+// follow the reference's generic fills: cont copies the edge cell
+// (src/gradops.cu:947-1060), symm/asymm mirror (src/gradops.cu:1325-1465) about
+// the face between cells 1 and 2 in 2D and about cell 2 in 3D (the contcd4
+// pattern), asymm with the sign flipped; fixed ghost cells are never written
+// and keep the values they had when the state was set.
+inline void set_boundaries(KParams& K, const smaug_params_t* p, int nd) {
+  for (int d = 0; d < 3; d++) {
+    const int t = d < nd ? p->boundtype[d][0] : SMAUG_BC_PERIODIC;
+    K.bt[d] = t;
+    K.bc[d] = (t == SMAUG_BC_SYMM || t == SMAUG_BC_ASYMM) ? (nd == 3 ? SMAUG_BC_CONTCD4 : SMAUG_BC_SYMM) : t;
+    K.gneg[d] = (t == SMAUG_BC_ASYMM) ? 1 : 0;
+    K.cmax_floor[d] = 0.0;
+  }
+}
+
+inline bool has_fixed(const KParams& K) {
+  return K.bc[0] == SMAUG_BC_FIXED || K.bc[1] == SMAUG_BC_FIXED || K.bc[2] == SMAUG_BC_FIXED;
+}
 
 struct KBufs {
   const void* uin;     // [P][ncell] stage input, ghosts valid (double; float in the mixed form)

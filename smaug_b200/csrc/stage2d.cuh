@@ -528,7 +528,7 @@ __device__ __forceinline__ void stage2d_body(const KParams& P, const KBufs& B, i
   }
 
   // ---- combine, write, ghost images, CFL maxima -----------------------------
-  double cm0 = 0.0, cm1 = 0.0;
+  double cm0 = P.cmax_floor[0], cm1 = P.cmax_floor[1];
   if (active) {
     double res[6];
     const bool is_base = (MODE == SMAUG_INT_EULER) || B.stage == 3;
@@ -562,21 +562,28 @@ __device__ __forceinline__ void stage2d_body(const KParams& P, const KBufs& B, i
     iy[0] = gj;
     const int nx = 1 + ghost_images(gi, n0, P.bc[0], ix + 1);
     const int ny = 1 + ghost_images(gj, n1, P.bc[1], iy + 1);
+    bool negated = false;  // res holds the negated values
     for (int b = 0; b < ny; b++)
       for (int a2 = 0; a2 < nx; a2++) {
         const long cc = (long)iy[b] * n0 + ix[a2];
+        // antisymmetric images carry the opposite sign (negation is exact)
+        const bool neg = ((a2 > 0) && P.gneg[0]) != ((b > 0) && P.gneg[1]);
+        if (neg != negated) {
 #pragma unroll
-        for (int f = 0; f < 6; f++) store_value<MIX>(B, f * nc + cc, res[f], is_base);
+          for (int f = 0; f < 6; f++) res[f] = -res[f];
+          negated = neg;
+        }
+        const double* r = res;
+#pragma unroll
+        for (int f = 0; f < 6; f++) store_value<MIX>(B, f * nc + cc, r[f], is_base);
         double eb, rb, b1b, b2b;
         if (BG && a2 == 0 && b == 0) {
           eb = T.v(EB, lo); rb = T.v(RHOB, lo); b1b = T.v(BB1, lo); b2b = T.v(BB2, lo);
         } else {
           eb = B.bg[0 * nc + cc]; rb = B.bg[1 * nc + cc]; b1b = B.bg[2 * nc + cc]; b2b = B.bg[3 * nc + cc];
         }
-        cm0 = dmax0(cm0, cfast2(P.gamma, res[RHO], res[M1], res[M2], res[EN], res[B1], res[B2], eb, rb,
-                                b1b, b2b, 0));
-        cm1 = dmax0(cm1, cfast2(P.gamma, res[RHO], res[M1], res[M2], res[EN], res[B1], res[B2], eb, rb,
-                                b1b, b2b, 1));
+        cm0 = dmax0(cm0, cfast2(P.gamma, r[RHO], r[M1], r[M2], r[EN], r[B1], r[B2], eb, rb, b1b, b2b, 0));
+        cm1 = dmax0(cm1, cfast2(P.gamma, r[RHO], r[M1], r[M2], r[EN], r[B1], r[B2], eb, rb, b1b, b2b, 1));
       }
   }
   __shared__ double red[NTHREADS / 32][2];

@@ -557,7 +557,7 @@ __global__ void __launch_bounds__(s3::NT, 3) stage3d_fast(const KParams P, const
   }
 
   // ---- combine, write, ghost images, CFL maxima -----------------------------
-  double cm[3] = {0.0, 0.0, 0.0};
+  double cm[3] = {P.cmax_floor[0], P.cmax_floor[1], P.cmax_floor[2]};
   if (active) {
     double res[8];
     const bool is_base = (MODE == SMAUG_INT_EULER) || B.stage == 3;
@@ -593,12 +593,21 @@ __global__ void __launch_bounds__(s3::NT, 3) stage3d_fast(const KParams P, const
     const int nx = 1 + ghost_images(gt[0], n[0], P.bc[0], ix + 1);
     const int ny = 1 + ghost_images(gt[1], n[1], P.bc[1], iy + 1);
     const int nz = 1 + ghost_images(gt[2], n[2], P.bc[2], iz + 1);
+    bool negated = false;  // res holds the negated values
     for (int cz = 0; cz < nz; cz++)
       for (int b = 0; b < ny; b++)
         for (int a2 = 0; a2 < nx; a2++) {
           const long cc = ((long)iz[cz] * n[1] + iy[b]) * n[0] + ix[a2];
+          // antisymmetric images carry the opposite sign (negation is exact)
+          const bool neg = (((a2 > 0) && P.gneg[0]) != ((b > 0) && P.gneg[1])) != ((cz > 0) && P.gneg[2]);
+          if (neg != negated) {
 #pragma unroll
-          for (int f = 0; f < 8; f++) store_value<MIX>(B, f * nc + cc, res[f], is_base);
+            for (int f = 0; f < 8; f++) res[f] = -res[f];
+            negated = neg;
+          }
+          const double* r = res;
+#pragma unroll
+          for (int f = 0; f < 8; f++) store_value<MIX>(B, f * nc + cc, r[f], is_base);
           double gg[5];
           if (a2 == 0 && b == 0 && cz == 0) {
 #pragma unroll
@@ -608,7 +617,7 @@ __global__ void __launch_bounds__(s3::NT, 3) stage3d_fast(const KParams P, const
             for (int f = 0; f < 5; f++) gg[f] = __ldg(B.bg + f * nc + cc);
           }
 #pragma unroll
-          for (int d = 0; d < 3; d++) cm[d] = dmax0(cm[d], cfast3(P.gamma, res, gg, d));
+          for (int d = 0; d < 3; d++) cm[d] = dmax0(cm[d], cfast3(P.gamma, r, gg, d));
         }
   }
   __shared__ double red[s3::NT / 32][3];

@@ -48,12 +48,17 @@ sys.path.insert(0, ROOT)
 WORK = os.path.join(HERE, "_inputs")          # git-ignored; travels to the GPU box
 RUNS = os.path.join(ROOT, "gpurun_out", "gold")
 
-# name: (nx, ny, seed, NT, steps kept)
+# name: (nx, ny, seed, NT, steps kept[, boundary types per dim])
 CASES = {
     "g16": (16, 16, 11, 21, [1, 2, 3, 5, 10, 20]),
     "g18x12": (18, 12, 12, 21, [1, 2, 3, 5, 10, 20]),
     "ot64": (64, 64, 1, 12, [1, 11]),
     "ot24x20": (24, 20, 5, 12, [0, 1, 2, 3, 4, 5]),
+    # fixed (5) ghosts: the OT model's cuboundary (src/boundary.cu:231-252)
+    # dispatches periodic only, so type 5 leaves the ghost layers as read
+    # from the .ini; the gradient edge zeroing of non-periodic types applies
+    "f16x": (16, 16, 13, 21, [1, 2, 3, 5, 10, 20], (5, 0)),
+    "f18y": (18, 12, 14, 21, [1, 2, 3, 5, 10, 20], (0, 5)),
 }
 GAMMA_REF = 1.66666667  # models/iosmaugparams.h.ot PGAMMA
 
@@ -138,10 +143,11 @@ def prepare():
     from smaug_b200 import formats
     from oracle import build_ref
     os.makedirs(WORK, exist_ok=True)
-    for name, (nx, ny, seed, nt, keep) in _selected(CASES).items():
+    for name, case in _selected(CASES).items():
+        nx, ny, seed, nt, keep = case[:5]
         w, pos = ot_state(nx, ny, seed)
         formats.write_ini(os.path.join(WORK, name + ".ini"), w, pos)
-        build_ref.build_ref(name, nx, ny, nt, verbose=False)
+        build_ref.build_ref(name, nx, ny, nt, verbose=False, **_bc_defines(case))
         print("prepared", name)
     for name, ((nx, ny, nz), seed, nt, keep, runs) in _selected(CASES3).items():
         w, pos = tube_state(nx, ny, nz, seed)
@@ -165,9 +171,19 @@ def _run_one(name, keep, tag=""):
         sys.exit(rc)
 
 
+def _bc_defines(case):
+    if len(case) < 6:
+        return {}
+    out = {}
+    for d, t in enumerate(case[5]):
+        out["BCU%d" % d] = str(t)
+        out["BCL%d" % d] = str(t)
+    return out
+
+
 def run():
-    for name, (nx, ny, seed, nt, keep) in _selected(CASES).items():
-        _run_one(name, keep)
+    for name, case in _selected(CASES).items():
+        _run_one(name, case[4])
     for name, (n, seed, nt, keep, runs) in _selected(CASES3).items():
         for r in range(runs):
             _run_one(name, keep, "" if r == 0 else "_r%d" % r)
@@ -188,7 +204,9 @@ def collect():
                             dx=np.array([L3 / nx, L3 / ny, L3 / nz]),
                             g=np.array([G3, 0.0, 0.0]))
         print("wrote", name)
-    for name, (nx, ny, seed, nt, keep) in _selected(CASES).items():
+    for name, case in _selected(CASES).items():
+        nx, ny, seed, nt, keep = case[:5]
+        bt = case[5] if len(case) > 5 else (0, 0)
         w0, pos0, _ = formats.read_ini(os.path.join(WORK, name + ".ini"), 2)
         states, times = [], []
         for k in keep:
@@ -198,7 +216,8 @@ def collect():
         np.savez_compressed(os.path.join(HERE, name + ".npz"), w0=w0[:6], pos=pos0,
                             steps=np.array(keep), states=np.array(states),
                             hdr_t=np.array(times), gamma=GAMMA_REF,
-                            dx=np.array([2 * math.pi / nx, 2 * math.pi / ny]))
+                            dx=np.array([2 * math.pi / nx, 2 * math.pi / ny]),
+                            bt=np.array(bt))
         print("wrote", name)
 
 

@@ -7,6 +7,7 @@ from smaug_b200 import params as P
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 STRICT = ("g16", "g18x12", "ot64")     # full multi-step runs
+BOUNDARY = ("f16x", "f18y")            # fixed ghosts along dim 0 / dim 1
 ONESTEP = ("ot24x20",)                 # consecutive steps, one-step parity
 STRICT3 = ("t3s", "t3a", "t3b")        # 3D flux-tube build, contcd4 ghosts, backgrounds
 
@@ -31,6 +32,8 @@ def params(d, **kw):
                              gamma=float(d["gamma"]), courant=0.3, dtmax=1.0, dt=1e-8,
                              g=tuple(d["g"]), boundtype=[[P.BC_CONTCD4] * 2] * 3, **kw)
     ny, nx = d["w0"].shape[1:]
+    if "bt" in d:
+        kw.setdefault("boundtype", tuple(int(b) for b in d["bt"]))
     return P.make_params(ndim=2, n=(nx, ny, 1), dx=tuple(d["dx"]), gamma=float(d["gamma"]),
                          courant=0.3, dtmax=1.0, dt=1e-8, **kw)
 

@@ -43,6 +43,12 @@ CASES = [
     (40, 40, 5, {"boundtype": (P.BC_CONTCD4, P.BC_CONTCD4)}),
     (40, 40, 5, {"boundtype": (P.BC_CONT, P.BC_PERIODIC)}),
     (40, 40, 5, {"boundtype": (P.BC_SYMM, P.BC_CONTCD4)}),
+    (40, 40, 5, {"boundtype": (P.BC_FIXED, P.BC_PERIODIC)}),
+    (36, 40, 5, {"boundtype": (P.BC_PERIODIC, P.BC_FIXED)}),
+    (40, 38, 5, {"boundtype": (P.BC_FIXED, P.BC_CONTCD4)}),
+    (33, 30, 4, {"boundtype": (P.BC_FIXED, P.BC_FIXED)}),
+    (38, 34, 5, {"boundtype": (P.BC_SYMM, P.BC_FIXED)}),
+    (34, 38, 5, {"boundtype": (P.BC_FIXED, P.BC_CONT)}),
     (40, 40, 5, {"g": (-0.3, 0.2)}),
     (40, 40, 5, {"pad_model": P.PAD_ZERO}),
     (40, 40, 5, {"hyperdifmom": 0}),
@@ -106,3 +112,67 @@ def test_large_grid_against_oracle(engine_lib, oracle):
     p = params_for(w, dx)
     got, _, _, ref = run_both(engine_lib, oracle, w, pos, p, 2)
     assert_parity(got, ref)
+
+
+def small_perturbation(w, scale=0.01):
+    """Evolved fields scaled down on top of large backgrounds, so that the
+    negated images of antisymmetric boundaries keep the total density and
+    energy positive."""
+    w = w.copy()
+    ny, nx = w.shape[1:]
+    w[:6] *= scale
+    w[6] = 2.0
+    w[7] = 1.0
+    w[8] = 0.1
+    w[9] = 0.05
+    return w
+
+
+@pytest.mark.parametrize("integ", [P.INT_EULER, P.INT_RK4])
+@pytest.mark.parametrize("bt", [(P.BC_ASYMM, P.BC_PERIODIC), (P.BC_CONTCD4, P.BC_ASYMM),
+                                (P.BC_ASYMM, P.BC_CONT), (P.BC_SYMM, P.BC_ASYMM)])
+def test_parity_antisymmetric(engine_lib, oracle, bt, integ):
+    """Antisymmetric ghosts (src/gradops.cu:1397-1465) alone and beside the
+    other types, corners included."""
+    w, pos, dx = ot_rect(34, 30, seed=17)
+    w = small_perturbation(w)
+    p = params_for(w, dx, integrator=integ, boundtype=bt)
+    got, (it, t, dt), _, ref = run_both(engine_lib, oracle, w, pos, p, 5)
+    assert_parity(got, ref)
+    assert abs(dt - ref.dt) <= 1e-13 * abs(ref.dt)
+
+
+@pytest.mark.parametrize("integ", [P.INT_EULER, P.INT_RK4])
+def test_fixed_ghosts_keep_initial_values(engine_lib, integ):
+    """Fixed boundaries: the two ghost layers along that dimension (corners
+    included) hold the initial values after any number of steps."""
+    w, pos, dx = ot_rect(30, 26, seed=8)
+    p = params_for(w, dx, integrator=integ, boundtype=(P.BC_FIXED, P.BC_PERIODIC))
+    e = engine_lib.Engine(p, w, pos)
+    e.step(7)
+    got = e.state()
+    e.close()
+    for f in range(6):
+        for cols in (slice(0, 2), slice(-2, None)):
+            assert np.array_equal(got[f][2:-2, cols], w[f][2:-2, cols])
+    # corners: the periodic images of the fixed columns
+    ny = w.shape[1]
+    for f in range(6):
+        assert np.array_equal(got[f][0:2, 0:2], w[f][ny - 4:ny - 2, 0:2])
+        assert np.array_equal(got[f][ny - 2:, -2:], w[f][2:4, -2:])
+
+
+def test_fixed_with_ghost_updates_is_rejected(engine_lib):
+    """The reference's driver (every cell), 2D gravity and 2D background
+    energy coupling also update ghost cells, which fixed boundaries would then
+    keep: those combinations are refused instead of silently differing."""
+    w, pos, dx = ot_rect(20, 20, seed=2)
+    bt = (P.BC_FIXED, P.BC_PERIODIC)
+    for kw in (dict(driver=P.DRIVER_GAUSS, drv_amp=0.1, drv_x0=(1.0, 1.0, 0.0),
+                    drv_sigma=(0.5, 0.5, 0.0)), dict(g=(0.2, 0.0))):
+        with pytest.raises(Exception, match="fixed"):
+            engine_lib.Engine(params_for(w, dx, boundtype=bt, **kw), w, pos)
+    wb = with_background(w)
+    with pytest.raises(Exception, match="fixed"):
+        engine_lib.Engine(params_for(wb, dx, boundtype=bt), wb, pos)
+

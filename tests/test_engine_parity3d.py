@@ -15,6 +15,7 @@ pytestmark = pytest.mark.gpu
 TOL = 1e-12
 
 C4, PER, CONT, SYM = P.BC_CONTCD4, P.BC_PERIODIC, P.BC_CONT, P.BC_SYMM
+FIX, ASYM = P.BC_FIXED, P.BC_ASYMM
 
 
 def run_both(engine_lib, oracle, w, pos, p, steps):
@@ -48,6 +49,9 @@ CASES = [
     (10, 12, 7, 4, True, {"chyp": [0.3, 0.1, 0.25, 0.2, 0.15, 0.05, 0.12, 0.18, 0, 0, 0, 0, 0]}),
     (10, 10, 8, 4, True, {"moddton": 0, "dt": 1e-3}),
     (10, 10, 8, 4, True, {"dtmax": 5e-4}),                     # CFL candidate rejected
+    (12, 10, 8, 4, True, {"boundtype": (FIX, PER, C4)}),
+    (9, 10, 7, 4, True, {"boundtype": (ASYM, FIX, PER)}),
+    (10, 8, 9, 4, True, {"boundtype": (C4, ASYM, SYM)}),
 ]
 
 

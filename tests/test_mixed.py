@@ -69,6 +69,21 @@ def test_mixed_background_2d(engine_lib, oracle, integ):
 
 
 @pytest.mark.parametrize("integ", [P.INT_RK4, P.INT_EULER])
+def test_mixed_fixed_and_antisymmetric(engine_lib, oracle, integ):
+    """Fixed ghosts live in every float buffer; antisymmetric images."""
+    w, pos, dx = ot_rect(40, 36, seed=6)
+    p = params_for(w, dx, integrator=integ, precision=P.PREC_MIXED,
+                   boundtype=(P.BC_FIXED, P.BC_PERIODIC))
+    errs, _, _ = errors(engine_lib, oracle, w, pos, p, 20, 6)
+    assert max(errs) <= TOL, errs
+    w3, pos3, dx3 = state3d(10, 9, 8, seed=9)
+    p3 = params3(w3, dx3, integrator=integ, precision=P.PREC_MIXED,
+                 boundtype=(P.BC_ASYMM, P.BC_FIXED, P.BC_PERIODIC))
+    errs, _, _ = errors(engine_lib, oracle, w3, pos3, p3, 10, 8)
+    assert max(errs) <= TOL, errs
+
+
+@pytest.mark.parametrize("integ", [P.INT_RK4, P.INT_EULER])
 def test_mixed_3d(engine_lib, oracle, integ):
     w, pos, dx = state3d(16, 12, 10, seed=7)
     p = params3(w, dx, integrator=integ, g=(-0.1, 0, 0), precision=P.PREC_MIXED,
