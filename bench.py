@@ -288,11 +288,15 @@ def adjoint_main(args):
     through the hand-written adjoint with checkpoints every 20 steps; the
     target comes from a forward run with seed-shifted parameters.  Reports the
     forward and forward+backward times (CUDA events), their ratio, and the
-    central finite-difference check (h = 1e-4 relative) of every component."""
+    central finite-difference check (h = 1e-4 relative) of every component,
+    for the taped rollout and (composed_checkpoint_autograd) for single-step
+    Functions under torch.utils.checkpoint.  No driver signal reaches the
+    3 Mm row within 400 steps of half the CFL dt (the loss there is exactly
+    0), so the same measurement is repeated for the row at 0.4 Mm."""
     import numpy as np
     import torch
     from smaug_b200 import engine, params as P
-    from smaug_b200.adjoint import StepAdjoint, rollout
+    from smaug_b200.adjoint import StepAdjoint, rollout, rollout_autograd
     nsteps = args.adj_steps
     p, w, pos = make_slab()
     e = engine.Engine(p, w, pos)
@@ -304,11 +308,29 @@ def adjoint_main(args):
     q.dt = 0.5 * dt
     sa = StepAdjoint(q, w, pos)
     u0 = torch.tensor(w[:6], dtype=torch.float64, device="cuda").contiguous()
-    kz = int(np.argmin(np.abs(pos[0][0] - args.obs_z)))
     rhob = torch.tensor(w[7], device="cuda", dtype=torch.float64)
     theta0 = torch.tensor([200.0, 30.0, 1.0e6], dtype=torch.float64)
     rng = np.random.default_rng(12)
     shift = torch.tensor(1.0 + 0.05 * rng.standard_normal(3), dtype=torch.float64)
+    line = None
+    for obs_z in [args.obs_z] + ([0.4e6] if abs(args.obs_z - 0.4e6) > 1.0 else []):
+        res = _adjoint_case(args, sa, q, p, u0, pos, rhob, theta0, shift, obs_z, nsteps,
+                            rollout, rollout_autograd)
+        if line is None:
+            line = res
+        else:
+            line["observation_row_0p4Mm"] = {k: res[k] for k in (
+                "value", "loss", "grad", "fd", "fd_rel_err", "forward_ms", "forward_backward_ms")}
+            line["observation_row_0p4Mm"]["config_observed_row_z_m"] = res["config"]["observed_row_z_m"]
+    sa.close()
+    print(json.dumps(line), flush=True)
+
+
+def _adjoint_case(args, sa, q, p, u0, pos, rhob, theta0, shift, obs_z, nsteps, rollout,
+                  rollout_autograd):
+    import numpy as np
+    import torch
+    kz = int(np.argmin(np.abs(pos[0][0] - obs_z)))
 
     def vz_row(u):
         return u[1, :, kz] / (u[0, :, kz] + rhob[:, kz])
@@ -336,6 +358,11 @@ def adjoint_main(args):
     for _ in range(max(args.warmup, 1)):
         with torch.no_grad():
             rollout(sa, theta0, u0, 20, loss_fn, checkpoint_every=20)
+    # one short backward of each rollout outside the timed regions (the tape
+    # of 20 steps is allocated on the first backward)
+    for fn in (rollout, rollout_autograd):
+        thw = theta0.clone().requires_grad_(True)
+        fn(sa, thw, u0, 20, loss_fn, checkpoint_every=20).backward()
     with torch.no_grad():
         L0, ms_fwd = timed(lambda: rollout(sa, theta0, u0, nsteps, loss_fn, checkpoint_every=20))
 
@@ -346,6 +373,14 @@ def adjoint_main(args):
         return th.grad.clone()
 
     grad, ms_fb = timed(fwd_bwd)
+
+    def fwd_bwd_composed():
+        th = theta0.clone().requires_grad_(True)
+        L = rollout_autograd(sa, th, u0, nsteps, loss_fn, checkpoint_every=20)
+        L.backward()
+        return th.grad.clone()
+
+    grad_c, ms_fb_c = timed(fwd_bwd_composed)
     fd = []
     for k in range(3):
         h = 1e-4 * float(theta0[k])
@@ -357,7 +392,6 @@ def adjoint_main(args):
                 vals.append(float(rollout(sa, th, u0, nsteps, loss_fn, checkpoint_every=20)))
         fd.append((vals[0] - vals[1]) / (2 * h))
     rel = [abs(float(grad[k]) - fd[k]) / max(abs(fd[k]), 1e-300) for k in range(3)]
-    sa.close()
     cells = p.interior_cells()
     line = {
         "metric": "adjoint cost / forward cost (loss gradient over a 400-step RK4 rollout)",
@@ -370,8 +404,13 @@ def adjoint_main(args):
         "forward_ms": ms_fwd, "forward_backward_ms": ms_fb,
         "forward_mcell_updates_per_s": cells * nsteps / (ms_fwd / 1e3) / 1e6,
         "loss": float(L0), "grad": [float(g) for g in grad], "fd": fd, "fd_rel_err": rel,
+        "composed_checkpoint_autograd": {
+            "value": ms_fb_c / ms_fwd, "forward_backward_ms": ms_fb_c,
+            "grad": [float(g) for g in grad_c],
+            "note": "single-step Functions under torch.utils.checkpoint; each step adjoint "
+                    "recomputes its stage inputs"},
     }
-    print(json.dumps(line), flush=True)
+    return line
 
 
 def dist_setup(args):

@@ -217,6 +217,16 @@ int smaug_adj_forward(smaug_adj_t a, const double* u, double* u_next, double t, 
    arrays, overwritten); recomputes the step's stages; enqueued on `stream` */
 int smaug_adj_backward(smaug_adj_t a, const double* u, const double* ubar_next, double* ubar,
                        double* thbar, double t, void* stream);
+/* Tape of nslots steps (4 x 6 x ncells doubles each): a taped forward keeps
+   the step's stage inputs, so the matching backward recomputes nothing.
+   Grows only (waits for the device when it reallocates). */
+int smaug_adj_tape_reserve(smaug_adj_t a, int32_t nslots);
+/* smaug_adj_forward, keeping the stage inputs in tape slot `slot` */
+int smaug_adj_forward_tape(smaug_adj_t a, const double* u, double* u_next, double t, int32_t slot,
+                           void* stream);
+/* smaug_adj_backward of the step taped in `slot` (same t) */
+int smaug_adj_backward_tape(smaug_adj_t a, int32_t slot, const double* ubar_next, double* ubar,
+                            double* thbar, double t, void* stream);
 int smaug_adj_destroy(smaug_adj_t a);
 
 /* Message of the calling thread's last failure ("" if none). */

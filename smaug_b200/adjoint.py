@@ -5,8 +5,11 @@ checkpointed rollout.
 The step is u -> U' (2D, FP64, dt = params.dt held fixed, params.moddton = 0);
 its adjoint gives the gradients with respect to the state and to the driver
 parameters theta = (amplitude, period, centre along dim 1).  A rollout of N
-steps keeps only every `checkpoint_every`-th state and recomputes the states
-inside a segment during the backward pass (torch.utils.checkpoint).
+steps keeps only every `checkpoint_every`-th state; the backward pass
+recomputes one segment at a time into a device tape of the segment's stage
+inputs, then runs the step adjoints from the tape (`rollout`).  The same
+gradient composed from single-step Functions with torch.utils.checkpoint is
+`rollout_autograd`.
 States are CUDA float64 tensors of the evolved fields, shape (6, n1, n0); the
 background fields come from the state given at construction.
 """
@@ -59,6 +62,25 @@ class StepAdjoint:
             float(t), ctypes.c_void_p(st)))
         return ubar, thbar
 
+    def reserve(self, nslots):
+        _engine._check(_engine.lib().smaug_adj_tape_reserve(self.h, int(nslots)))
+
+    def forward_tape(self, u, t, slot):
+        out = torch.empty_like(u)
+        st = torch.cuda.current_stream(u.device).cuda_stream
+        _engine._check(_engine.lib().smaug_adj_forward_tape(self.h, self._ptr(u), self._ptr(out), float(t),
+                                                            int(slot), ctypes.c_void_p(st)))
+        return out
+
+    def backward_tape(self, slot, ubar_next, t):
+        ubar = torch.empty_like(ubar_next)
+        thbar = torch.empty(3, dtype=torch.float64, device=ubar_next.device)
+        st = torch.cuda.current_stream(ubar_next.device).cuda_stream
+        _engine._check(_engine.lib().smaug_adj_backward_tape(
+            self.h, int(slot), self._ptr(ubar_next.contiguous()), self._ptr(ubar), self._ptr(thbar),
+            float(t), ctypes.c_void_p(st)))
+        return ubar, thbar
+
     def close(self):
         if getattr(self, "h", None):
             _engine.lib().smaug_adj_destroy(self.h)
@@ -92,10 +114,72 @@ class Step(torch.autograd.Function):
         return thbar.to(theta.device, theta.dtype), ubar, None, None
 
 
+class _Rollout(torch.autograd.Function):
+    """L = sum_n loss_fn(u_n, n) over a rollout, with the hand-written step
+    adjoint applied segment by segment from a tape."""
+
+    @staticmethod
+    def forward(ctx, theta, u0, sa, nsteps, loss_fn, t0, every):
+        dt = sa.dt
+        sa.set_driver(*theta.detach().cpu().tolist())
+        ckpt = []
+        total = torch.zeros((), dtype=torch.float64, device=u0.device)
+        u = u0.detach()
+        with torch.no_grad():
+            for n in range(nsteps):
+                if n % every == 0:
+                    ckpt.append(u)
+                u = sa.forward(u, t0 + n * dt)
+                total = total + loss_fn(u, n + 1)
+        ctx.sa, ctx.nsteps, ctx.loss_fn, ctx.t0, ctx.every = sa, nsteps, loss_fn, t0, every
+        ctx.ckpt = ckpt
+        ctx.theta = theta.detach().cpu().tolist()
+        ctx.theta_meta = (theta.dtype, theta.device)
+        return total
+
+    @staticmethod
+    def backward(ctx, gL):
+        sa, nsteps, every, t0 = ctx.sa, ctx.nsteps, ctx.every, ctx.t0
+        dt = sa.dt
+        sa.set_driver(*ctx.theta)
+        sa.reserve(min(every, nsteps))
+        ubar = None
+        thbar = torch.zeros(3, dtype=torch.float64, device=gL.device)
+        for si in range(len(ctx.ckpt) - 1, -1, -1):
+            s = si * every
+            e = min(nsteps, s + every)
+            states = [ctx.ckpt[si]]
+            with torch.no_grad():
+                for n in range(s, e):
+                    states.append(sa.forward_tape(states[-1], t0 + n * dt, n - s))
+            for n in range(e - 1, s - 1, -1):
+                # d loss_fn(u_{n+1}, n+1) / d u_{n+1}
+                with torch.enable_grad():
+                    un = states[n - s + 1].detach().requires_grad_(True)
+                    gl, = torch.autograd.grad(ctx.loss_fn(un, n + 1), un, allow_unused=True)
+                g = gl * gL if gl is not None else torch.zeros_like(un)
+                ubar = g if ubar is None else ubar + g
+                ubar, tb = sa.backward_tape(n - s, ubar, t0 + n * dt)
+                thbar = thbar + tb
+        dtype, device = ctx.theta_meta
+        # ubar and thbar already carry the factor gL (it scales every loss gradient)
+        return thbar.to(device=device, dtype=dtype), ubar, None, None, None, None, None
+
+
 def rollout(sa, theta, u0, nsteps, loss_fn, t0=0.0, checkpoint_every=20):
     """sum over steps n = 1..nsteps of loss_fn(u_n, n), differentiable in
-    theta and u0; the states inside each segment of `checkpoint_every` steps
-    are recomputed in the backward pass."""
+    theta and u0.  Keeps every `checkpoint_every`-th state; the backward
+    recomputes each segment once into a tape of its stage inputs
+    (smaug_adj_forward_tape) and applies the step adjoints from it
+    (smaug_adj_backward_tape), so no step is computed more than twice."""
+    return _Rollout.apply(theta, u0, sa, nsteps, loss_fn, t0, max(1, int(checkpoint_every)))
+
+
+def rollout_autograd(sa, theta, u0, nsteps, loss_fn, t0=0.0, checkpoint_every=20):
+    """The same sum composed from single-step Functions (Step) under
+    torch.utils.checkpoint: the states inside each segment of
+    `checkpoint_every` steps are recomputed in the backward pass, and each
+    step adjoint recomputes its stage inputs."""
     dt = sa.dt
 
     def segment(theta_, u_, n0, n1):

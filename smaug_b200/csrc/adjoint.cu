@@ -43,6 +43,9 @@ namespace smaug {
 namespace {
 
 constexpr int ANT = TX * TY;  // threads per adjoint block (tile 32x8 as the forward)
+#ifndef SMAUG_ADJ_MINB
+#define SMAUG_ADJ_MINB 2  // resident blocks per SM the adjoint stage is compiled for
+#endif
 
 struct A2 {
   double* S;   // [6][RC] state
@@ -500,7 +503,7 @@ __device__ __forceinline__ double w4(int k) {
   return k == 1 ? 8.0 / 6.0 : (k == -1 ? -8.0 / 6.0 : (k == -2 ? 1.0 / 6.0 : (k == 2 ? -1.0 / 6.0 : 0.0)));
 }
 
-__global__ void __launch_bounds__(ANT, 2) adj_stage2d(const KParams P, const AdjIn I) {
+__global__ void __launch_bounds__(ANT, SMAUG_ADJ_MINB) adj_stage2d(const KParams P, const AdjIn I) {
   extern __shared__ double smem[];
   A2 T;
   T.S = smem;
@@ -736,57 +739,50 @@ __global__ void cmax_value2d(const KParams P, const double* X, const double* bg,
   }
 }
 
-__global__ void cmax_argmax2d(const KParams P, const double* X, const double* bg,
-                              const unsigned long long* mx, int* arg) {
+// the same for the four stage inputs of a step in one pass each
+struct X4 {
+  const double* x[4];
+};
+
+__global__ void cmax4_value2d(const KParams P, const X4 X, const double* bg, unsigned long long* mx) {
   const long c = blockIdx.x * (long)blockDim.x + threadIdx.x;
   const long nc = P.ncell;
-  if (c >= nc) return;
-  for (int d = 0; d < 2; d++) {
-    const double v = cfast2(P.gamma, X[c], X[nc + c], X[2 * nc + c], X[3 * nc + c], X[4 * nc + c],
-                            X[5 * nc + c], bg[c], bg[nc + c], bg[2 * nc + c], bg[3 * nc + c], d);
-    if (v == __longlong_as_double((long long)mx[d])) atomicMin(arg + d, (int)c);
+  double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  if (c < nc) {
+    const double g0 = bg[c], g1 = bg[nc + c], g2 = bg[2 * nc + c], g3 = bg[3 * nc + c];
+#pragma unroll
+    for (int s = 0; s < 4; s++) {
+      const double* x = X.x[s];
+#pragma unroll
+      for (int d = 0; d < 2; d++)
+        v[2 * s + d] = cfast2(P.gamma, x[c], x[nc + c], x[2 * nc + c], x[3 * nc + c], x[4 * nc + c],
+                              x[5 * nc + c], g0, g1, g2, g3, d);
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 8; k++) {
+    double w = v[k] > 0 ? v[k] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) w = dmax0(w, __shfl_xor_sync(0xffffffffu, w, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(mx + k, (unsigned long long)__double_as_longlong(w));
   }
 }
 
-// G^T: the adjoint of the ghost fill; every ghost cell's adjoint is added to
-// its source interior cell and cleared (gather over the ghost images)
-__global__ void ghost_fold2d(const KParams P, double* Xb) {
+__global__ void cmax4_argmax2d(const KParams P, const X4 X, const double* bg,
+                               const unsigned long long* mx, int* arg) {
   const long c = blockIdx.x * (long)blockDim.x + threadIdx.x;
   const long nc = P.ncell;
   if (c >= nc) return;
-  const int i = (int)(c % P.n0), j = (int)(c / P.n0);
-  if (i < 2 || i > P.n0 - 3 || j < 2 || j > P.n1 - 3) return;
-  int ix[3], iy[3];
-  ix[0] = i;
-  iy[0] = j;
-  const int nx = 1 + ghost_images(i, P.n0, P.bc[0], ix + 1);
-  const int ny = 1 + ghost_images(j, P.n1, P.bc[1], iy + 1);
-  if (nx == 1 && ny == 1) return;
-  for (int f = 0; f < 6; f++) {
-    double s = 0.0;
-    for (int b = 0; b < ny; b++)
-      for (int a = 0; a < nx; a++) {
-        if (a == 0 && b == 0) continue;
-        s += Xb[f * nc + (long)iy[b] * P.n0 + ix[a]];
-      }
-    Xb[f * nc + c] += s;
+  const double g0 = bg[c], g1 = bg[nc + c], g2 = bg[2 * nc + c], g3 = bg[3 * nc + c];
+#pragma unroll
+  for (int s = 0; s < 4; s++) {
+    const double* x = X.x[s];
+#pragma unroll
+    for (int d = 0; d < 2; d++) {
+      const double v = cfast2(P.gamma, x[c], x[nc + c], x[2 * nc + c], x[3 * nc + c], x[4 * nc + c],
+                              x[5 * nc + c], g0, g1, g2, g3, d);
+      if (v == __longlong_as_double((long long)mx[2 * s + d])) atomicMin(arg + 2 * s + d, (int)c);
+    }
   }
-}
-
-__global__ void ghost_clear2d(const KParams P, double* Xb) {
-  const long c = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  const long nc = P.ncell;
-  if (c >= nc) return;
-  const int i = (int)(c % P.n0), j = (int)(c / P.n0);
-  if (i >= 2 && i <= P.n0 - 3 && j >= 2 && j <= P.n1 - 3) return;
-  for (int f = 0; f < 6; f++) Xb[f * nc + c] = 0.0;
-}
-
-// y = a*x + b*y over n values (b == 0: y = a*x)
-__global__ void axpby(long n, double a, const double* x, double b, double* y) {
-  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  y[i] = (b == 0.0 ? 0.0 : b * y[i]) + a * x[i];
 }
 
 }  // namespace
@@ -801,6 +797,62 @@ __global__ void ghost_fill_adj2d(const KParams P, double* u) {
   if (si == i && sj == j) return;
   const long s = (long)sj * P.n0 + si;
   for (int f = 0; f < 6; f++) u[f * P.ncell + c] = u[f * P.ncell + s];
+}
+
+__global__ void set_dt_t(double* dtb, double* tb, double dt, double t) {
+  dtb[0] = dt;
+  dtb[1] = dt;
+  tb[0] = t;
+  tb[1] = t;
+}
+
+// G^T x at cell c: the value plus those of its ghost images (interior
+// cells), 0 at ghost cells
+__device__ __forceinline__ double fold_at(const KParams& P, const double* x, long c, int i, int j) {
+  if (i < 2 || i > P.n0 - 3 || j < 2 || j > P.n1 - 3) return 0.0;
+  int ix[3], iy[3];
+  ix[0] = i;
+  iy[0] = j;
+  const int nx = 1 + ghost_images(i, P.n0, P.bc[0], ix + 1);
+  const int ny = 1 + ghost_images(j, P.n1, P.bc[1], iy + 1);
+  double s = x[c];
+  if (nx == 1 && ny == 1) return s;
+  double g = 0.0;
+  for (int b = 0; b < ny; b++)
+    for (int a = 0; a < nx; a++) {
+      if (a == 0 && b == 0) continue;
+      g += x[(long)iy[b] * P.n0 + ix[a]];
+    }
+  return s + g;
+}
+
+// start of the backward: W = G^T ubar_next, ubar = W, k-bar_4 = W / 6
+__global__ void adj_head(const KParams P, const double* ubn, double* W, double* ubar, double* Kb, double w4) {
+  const long c = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  const long nc = P.ncell;
+  if (c >= nc) return;
+  const int i = (int)(c % P.n0), j = (int)(c / P.n0);
+  for (int f = 0; f < 6; f++) {
+    const double w = fold_at(P, ubn + f * nc, c, i, j);
+    W[f * nc + c] = w;
+    ubar[f * nc + c] = w;
+    Kb[f * nc + c] = w4 * w;
+  }
+}
+
+// end of stage s of the backward: t_s = G^T X-bar, ubar += t_s and (s > 0)
+// k-bar_{s-1} = wk W + half t_s
+__global__ void adj_tail(const KParams P, const double* Xb, const double* W, double* ubar, double* Kb,
+                         double wk, double half, int more) {
+  const long c = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  const long nc = P.ncell;
+  if (c >= nc) return;
+  const int i = (int)(c % P.n0), j = (int)(c / P.n0);
+  for (int f = 0; f < 6; f++) {
+    const double x = fold_at(P, Xb + f * nc, c, i, j);
+    ubar[f * nc + c] += x;
+    if (more) Kb[f * nc + c] = fma(half, x, wk * W[f * nc + c]);
+  }
 }
 }  // namespace
 
@@ -824,6 +876,8 @@ struct Adjoint {
   double* sbar = nullptr;              // [2]
   unsigned long long* mx = nullptr;    // [4][2] stage CFL maxima
   int* arg = nullptr;                  // [4][2] their cells
+  double* tape = nullptr;              // [nslots][4][6][nc] stage inputs of taped steps
+  int nslots = 0;
 };
 
 static void free_adj(Adjoint* a) {
@@ -846,6 +900,7 @@ static void free_adj(Adjoint* a) {
   cudaFree(a->sbar);
   cudaFree(a->mx);
   cudaFree(a->arg);
+  cudaFree(a->tape);
   delete a;
 }
 
@@ -967,22 +1022,22 @@ static int adj_create(const smaug_params_t* p, const double* w, const double* po
 #define G_LAUNCH(n) (unsigned)(((n) + 255) / 256), 256, 0, st
 
 // forward RK4 step: X[0] = G(u) ... X[3] = stage 4 input, X[4] = U'
-static int adj_fwd(Adjoint* a, const double* u, double t, cudaStream_t st) {
+// One RK4 step from u; the stage inputs go to Xs[0..3] (the handle's own
+// buffers or a tape slot), the result to X[4].
+static int adj_fwd(Adjoint* a, const double* u, double t, cudaStream_t st, double* const* Xs) {
   const long nc = a->nc;
   const size_t eb = sizeof(double) * 6 * nc;
-  CUDA_TRY(cudaMemcpyAsync(a->X[0], u, eb, cudaMemcpyDeviceToDevice, st));
-  ghost_fill_adj2d<<<G_LAUNCH(nc)>>>(a->K, a->X[0]);
+  CUDA_TRY(cudaMemcpyAsync(Xs[0], u, eb, cudaMemcpyDeviceToDevice, st));
+  ghost_fill_adj2d<<<G_LAUNCH(nc)>>>(a->K, Xs[0]);
   CUDA_TRY(cudaMemsetAsync(a->ring, 0, sizeof(unsigned long long) * 9, st));
-  cmax_value2d<<<G_LAUNCH(nc)>>>(a->K, a->X[0], a->bg, a->ring);
-  const double dt2[2] = {a->P.dt, a->P.dt}, t2[2] = {t, t};
-  CUDA_TRY(cudaMemcpyAsync(a->dtb, dt2, sizeof(dt2), cudaMemcpyHostToDevice, st));
-  CUDA_TRY(cudaMemcpyAsync(a->tb, t2, sizeof(t2), cudaMemcpyHostToDevice, st));
+  cmax_value2d<<<G_LAUNCH(nc)>>>(a->K, Xs[0], a->bg, a->ring);
+  set_dt_t<<<1, 1, 0, st>>>(a->dtb, a->tb, a->P.dt, t);
   CUDA_TRY(cudaGetLastError());
   for (int s = 0; s < 4; s++) {
     KBufs B{};
-    B.uin = a->X[s];
-    B.un = a->X[0];
-    B.uout = a->X[s + 1];
+    B.uin = Xs[s];
+    B.un = Xs[0];
+    B.uout = s < 3 ? Xs[s + 1] : a->X[4];
     B.acc = a->acc;
     B.bg = a->bg;
     for (int d = 0; d < 2; d++) {
@@ -1005,36 +1060,35 @@ static int adj_fwd(Adjoint* a, const double* u, double t, cudaStream_t st) {
   return SMAUG_OK;
 }
 
+// The adjoint of one step from u.  Xs: the step's stage inputs from a tape
+// slot, or null to recompute them from u.
 static int adj_bwd(Adjoint* a, const double* u, const double* ubar_next, double* ubar, double* thbar,
-                   double t, cudaStream_t st) {
-  int rc = adj_fwd(a, u, t, st);
-  if (rc) return rc;
-  const long nc = a->nc, n6 = 6 * nc;
-  const size_t eb = sizeof(double) * n6;
+                   double t, cudaStream_t st, double* const* Xs) {
+  if (!Xs) {
+    int rc = adj_fwd(a, u, t, st, a->X);
+    if (rc) return rc;
+    Xs = a->X;
+  }
+  const long nc = a->nc;
+  const size_t eb = sizeof(double) * 6 * nc;
   // CFL maxima of the four stage inputs and the cells that attain them
   CUDA_TRY(cudaMemsetAsync(a->mx, 0, sizeof(unsigned long long) * 8, st));
   CUDA_TRY(cudaMemsetAsync(a->arg, 0x7f, sizeof(int) * 8, st));
-  for (int s = 0; s < 4; s++) {
-    cmax_value2d<<<G_LAUNCH(nc)>>>(a->K, a->X[s], a->bg, a->mx + 2 * s);
-    cmax_argmax2d<<<G_LAUNCH(nc)>>>(a->K, a->X[s], a->bg, a->mx + 2 * s, a->arg + 2 * s);
-  }
-  // W = G^T ubar_next; ubar = W
-  CUDA_TRY(cudaMemcpyAsync(a->W, ubar_next, eb, cudaMemcpyDeviceToDevice, st));
-  ghost_fold2d<<<G_LAUNCH(nc)>>>(a->K, a->W);
-  ghost_clear2d<<<G_LAUNCH(nc)>>>(a->K, a->W);
-  CUDA_TRY(cudaMemcpyAsync(ubar, a->W, eb, cudaMemcpyDeviceToDevice, st));
-  CUDA_TRY(cudaMemsetAsync(thbar, 0, sizeof(double) * 3, st));
+  const X4 x4{{Xs[0], Xs[1], Xs[2], Xs[3]}};
+  cmax4_value2d<<<G_LAUNCH(nc)>>>(a->K, x4, a->bg, a->mx);
+  cmax4_argmax2d<<<G_LAUNCH(nc)>>>(a->K, x4, a->bg, a->mx, a->arg);
   const double wk[4] = {1.0 / 6.0, 1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0};  // k-bar = wk W + ...
   const double half[4] = {0.0, 0.5, 0.5, 1.0};   // X_s = U + half[s] k_{s-1}
+  // W = G^T ubar_next; ubar = W; k-bar of stage 4 = W / 6
+  adj_head<<<G_LAUNCH(nc)>>>(a->K, ubar_next, a->W, ubar, a->Kb, wk[3]);
+  CUDA_TRY(cudaMemsetAsync(thbar, 0, sizeof(double) * 3, st));
   const double dt = a->P.dt;
   const double ts[4] = {t, t + 0.5 * dt, t + 0.5 * dt, t + dt};
-  // k-bar of stage 4 = W / 6
-  axpby<<<G_LAUNCH(n6)>>>(n6, wk[3], a->W, 0.0, a->Kb);
   for (int s = 3; s >= 0; s--) {
     CUDA_TRY(cudaMemsetAsync(a->Xb, 0, eb, st));
     CUDA_TRY(cudaMemsetAsync(a->sbar, 0, sizeof(double) * 2, st));
     AdjIn I{};
-    I.X = a->X[s];
+    I.X = Xs[s];
     I.bg = a->bg;
     I.lam = a->Kb;
     I.Xb = a->Xb;
@@ -1050,18 +1104,19 @@ static int adj_bwd(Adjoint* a, const double* u, const double* ubar_next, double*
     I.tstage = ts[s];
     dim3 grid((a->K.n0 - 4 + TX - 1) / TX, (a->K.n1 - 4 + TY - 1) / TY);
     adj_stage2d<<<grid, dim3(TX, TY), adj_smem(), st>>>(a->K, I);
-    adj_cmax2d<<<1, 32, 0, st>>>(a->K, a->X[s], a->bg, a->arg + 2 * s, a->sbar, a->Xb);
-    ghost_fold2d<<<G_LAUNCH(nc)>>>(a->K, a->Xb);
-    ghost_clear2d<<<G_LAUNCH(nc)>>>(a->K, a->Xb);
-    CUDA_TRY(cudaGetLastError());
-    // ubar += t_s; k-bar of the previous stage = wk W + half[s] t_s
-    axpby<<<G_LAUNCH(n6)>>>(n6, 1.0, a->Xb, 1.0, ubar);
-    if (s > 0) {
-      axpby<<<G_LAUNCH(n6)>>>(n6, wk[s - 1], a->W, 0.0, a->Kb);
-      axpby<<<G_LAUNCH(n6)>>>(n6, half[s], a->Xb, 1.0, a->Kb);
-    }
+    adj_cmax2d<<<1, 32, 0, st>>>(a->K, Xs[s], a->bg, a->arg + 2 * s, a->sbar, a->Xb);
+    // t_s = G^T X-bar; ubar += t_s; k-bar of the previous stage = wk W + half[s] t_s
+    adj_tail<<<G_LAUNCH(nc)>>>(a->K, a->Xb, a->W, ubar, a->Kb, s > 0 ? wk[s - 1] : 0.0, half[s], s > 0);
     CUDA_TRY(cudaGetLastError());
   }
+  return SMAUG_OK;
+}
+
+// stage-input pointers of tape slot `slot`
+static int tape_slot(Adjoint* a, int slot, double** Xs) {
+  if (slot < 0 || slot >= a->nslots)
+    return set_error(SMAUG_E_INVALID, "tape slot %d outside [0, %d)", slot, a->nslots);
+  for (int s = 0; s < 4; s++) Xs[s] = a->tape + ((size_t)slot * 4 + s) * 6 * a->nc;
   return SMAUG_OK;
 }
 
@@ -1096,17 +1151,61 @@ extern "C" int smaug_adj_forward(smaug_adj_t h, const double* u, double* u_next,
   if (!h || !u || !u_next) return smaug::set_error(SMAUG_E_INVALID, "null argument");
   Adjoint* a = HA(h);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  int rc = smaug::adj_fwd(a, u, t, st);
+  int rc = smaug::adj_fwd(a, u, t, st, a->X);
   if (rc) return rc;
   CUDA_TRY(cudaMemcpyAsync(u_next, a->X[4], sizeof(double) * 6 * a->nc, cudaMemcpyDeviceToDevice, st));
   return SMAUG_OK;
+}
+
+extern "C" int smaug_adj_tape_reserve(smaug_adj_t h, int32_t nslots) {
+  smaug::clear_error();
+  if (!h || nslots < 0) return smaug::set_error(SMAUG_E_INVALID, "bad argument");
+  Adjoint* a = HA(h);
+  if (nslots <= a->nslots) return SMAUG_OK;
+  CUDA_TRY(cudaDeviceSynchronize());
+  cudaFree(a->tape);
+  a->tape = nullptr;
+  a->nslots = 0;
+  const size_t bytes = sizeof(double) * (size_t)nslots * 4 * 6 * a->nc;
+  if (cudaMalloc(&a->tape, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    a->tape = nullptr;
+    return smaug::set_error(SMAUG_E_NOMEM, "tape of %d steps (%zu bytes)", nslots, bytes);
+  }
+  a->nslots = nslots;
+  return SMAUG_OK;
+}
+
+extern "C" int smaug_adj_forward_tape(smaug_adj_t h, const double* u, double* u_next, double t,
+                                      int32_t slot, void* stream) {
+  smaug::clear_error();
+  if (!h || !u || !u_next) return smaug::set_error(SMAUG_E_INVALID, "null argument");
+  Adjoint* a = HA(h);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  double* Xs[4];
+  int rc = smaug::tape_slot(a, slot, Xs);
+  if (!rc) rc = smaug::adj_fwd(a, u, t, st, Xs);
+  if (rc) return rc;
+  CUDA_TRY(cudaMemcpyAsync(u_next, a->X[4], sizeof(double) * 6 * a->nc, cudaMemcpyDeviceToDevice, st));
+  return SMAUG_OK;
+}
+
+extern "C" int smaug_adj_backward_tape(smaug_adj_t h, int32_t slot, const double* ubar_next, double* ubar,
+                                       double* thbar, double t, void* stream) {
+  smaug::clear_error();
+  if (!h || !ubar_next || !ubar || !thbar) return smaug::set_error(SMAUG_E_INVALID, "null argument");
+  Adjoint* a = HA(h);
+  double* Xs[4];
+  int rc = smaug::tape_slot(a, slot, Xs);
+  if (rc) return rc;
+  return smaug::adj_bwd(a, nullptr, ubar_next, ubar, thbar, t, static_cast<cudaStream_t>(stream), Xs);
 }
 
 extern "C" int smaug_adj_backward(smaug_adj_t h, const double* u, const double* ubar_next, double* ubar,
                                   double* thbar, double t, void* stream) {
   smaug::clear_error();
   if (!h || !u || !ubar_next || !ubar || !thbar) return smaug::set_error(SMAUG_E_INVALID, "null argument");
-  return smaug::adj_bwd(HA(h), u, ubar_next, ubar, thbar, t, static_cast<cudaStream_t>(stream));
+  return smaug::adj_bwd(HA(h), u, ubar_next, ubar, thbar, t, static_cast<cudaStream_t>(stream), nullptr);
 }
 
 extern "C" int smaug_adj_destroy(smaug_adj_t h) {

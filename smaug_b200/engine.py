@@ -24,6 +24,7 @@ EXPORTS = [
     "smaug_batch_get_state", "smaug_batch_get_time", "smaug_batch_launch_shape",
     "smaug_batch_destroy", "smaug_batch_step_async", "smaug_batch_sync", "smaug_batch_set_stream",
     "smaug_adj_create", "smaug_adj_set_driver", "smaug_adj_forward", "smaug_adj_backward",
+    "smaug_adj_tape_reserve", "smaug_adj_forward_tape", "smaug_adj_backward_tape",
     "smaug_adj_destroy",
 ]
 
@@ -88,6 +89,9 @@ def lib():
         L.smaug_adj_set_driver.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_double]
         L.smaug_adj_forward.argtypes = [vp, vp, vp, ctypes.c_double, vp]
         L.smaug_adj_backward.argtypes = [vp, vp, vp, vp, vp, ctypes.c_double, vp]
+        L.smaug_adj_tape_reserve.argtypes = [vp, ctypes.c_int32]
+        L.smaug_adj_forward_tape.argtypes = [vp, vp, vp, ctypes.c_double, ctypes.c_int32, vp]
+        L.smaug_adj_backward_tape.argtypes = [vp, ctypes.c_int32, vp, vp, vp, ctypes.c_double, vp]
         L.smaug_adj_destroy.argtypes = [vp]
         _lib = L
     return _lib

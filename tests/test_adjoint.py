@@ -143,3 +143,34 @@ def test_adjoint_rejects(engine_lib):
     with pytest.raises(engine_lib.SmaugError) as e:
         StepAdjoint(p, w, pos)          # moddton = 1: dt would depend on the state
     assert e.value.code == 6
+
+
+def test_taped_rollout_equals_checkpointed_composition(engine_lib):
+    """rollout (segment recompute into a tape, step adjoints from the tape)
+    and rollout_autograd (single-step Functions under torch.utils.checkpoint,
+    each adjoint recomputing its stages) give the same loss and gradients
+    with respect to the parameters and the initial state."""
+    import torch
+    from smaug_b200.adjoint import rollout, rollout_autograd
+    sa, q, w, pos, u0 = setup(engine_lib, slab, 1)
+    kz = int(np.argmin(np.abs(pos[0][0] - 0.4e6)))
+    rhob = torch.tensor(w[7], device="cuda", dtype=torch.float64)
+    theta0 = torch.tensor([200.0, 30.0, 1.0e6], dtype=torch.float64)
+
+    def loss_fn(u, n):
+        v = u[1, :, kz] / (u[0, :, kz] + rhob[:, kz])
+        return (v ** 2).sum() * (1.0 + 0.1 * n)
+
+    out = []
+    for fn in (rollout, rollout_autograd):
+        th = theta0.clone().requires_grad_(True)
+        u = u0.clone().requires_grad_(True)
+        L = fn(sa, th, u, 9, loss_fn, checkpoint_every=4)
+        L.backward()
+        out.append((float(L), th.grad.clone(), u.grad.clone()))
+    (L1, g1, u1), (L2, g2, u2) = out
+    assert abs(L1 - L2) <= 1e-13 * abs(L2)
+    assert float((g1 - g2).abs().max()) <= 1e-10 * float(g2.abs().max())
+    assert float((u1 - u2).norm()) <= 1e-10 * float(u2.norm())
+    assert float(u2.norm()) > 0
+    sa.close()
