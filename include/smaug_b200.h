@@ -152,6 +152,12 @@ int smaug_set_stream(smaug_handle_t h, void* stream);
    Replaces cuupdate (src/update.cu:165-233). */
 int smaug_get_state(smaug_handle_t h, double* w);
 
+/* Copy fields [f0, f0+nf) of the current state (reference numbering) to the
+   host, field-major, w pointing at the destination of field f0 -- e.g. only
+   the evolved fields after a step.  A subset of smaug_get_state (cuupdate
+   copies every field of two slots, src/update.cu:207). */
+int smaug_get_fields(smaug_handle_t h, double* w, int32_t f0, int32_t nf);
+
 /* Replace the evolved fields from a host array in reference layout. */
 int smaug_set_state(smaug_handle_t h, const double* w);
 

@@ -724,6 +724,32 @@ extern "C" int smaug_get_state(smaug_handle_t h, double* w) {
   return SMAUG_OK;
 }
 
+extern "C" int smaug_get_fields(smaug_handle_t h, double* w, int32_t f0, int32_t nf) {
+  smaug::clear_error();
+  if (!h || !w) return smaug::set_error(SMAUG_E_INVALID, "null argument");
+  Engine* e = H(h);
+  const int nvar = e->nevo + e->nbg;
+  if (f0 < 0 || nf < 0 || f0 + nf > nvar)
+    return smaug::set_error(SMAUG_E_INVALID, "fields [%d, %d) outside [0, %d)", f0, f0 + nf, nvar);
+  if (nf == 0) return SMAUG_OK;
+  CUDA_TRY(cudaStreamSynchronize(e->stream));
+  const size_t nc = (size_t)e->ncell;
+  const int fe = f0 + nf < e->nevo ? f0 + nf : e->nevo;  // end of the evolved part
+  if (f0 < e->nevo) {
+    double* u = nullptr;
+    int rc = smaug::current_fp64(e, &u);
+    if (rc) return rc;
+    CUDA_TRY(cudaMemcpyAsync(w, u + (size_t)f0 * nc, sizeof(double) * (fe - f0) * nc,
+                             cudaMemcpyDeviceToHost, e->stream));
+  }
+  const int b0 = f0 > e->nevo ? f0 : e->nevo;
+  if (f0 + nf > e->nevo)
+    CUDA_TRY(cudaMemcpyAsync(w + (size_t)(b0 - f0) * nc, e->d_bg + (size_t)(b0 - e->nevo) * nc,
+                             sizeof(double) * (f0 + nf - b0) * nc, cudaMemcpyDeviceToHost, e->stream));
+  CUDA_TRY(cudaStreamSynchronize(e->stream));
+  return SMAUG_OK;
+}
+
 extern "C" int smaug_set_state(smaug_handle_t h, const double* w) {
   smaug::clear_error();
   if (!h || !w) return smaug::set_error(SMAUG_E_INVALID, "null argument");

@@ -16,7 +16,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIBPATH = os.path.join(HERE, "libsmaug_b200.so")
 
 EXPORTS = [
-    "smaug_params_default", "smaug_create", "smaug_step", "smaug_get_state",
+    "smaug_params_default", "smaug_create", "smaug_step", "smaug_get_state", "smaug_get_fields",
     "smaug_set_state", "smaug_get_time", "smaug_get_cmax", "smaug_write_out",
     "smaug_destroy", "smaug_last_error", "smaug_version", "smaug_read_ini",
     "smaug_write_out_host", "smaug_grid_metric", "smaug_step_async", "smaug_sync",
@@ -59,6 +59,7 @@ def lib():
         L.smaug_set_stream.argtypes = [vp, vp]
         L.smaug_euler_step_noalloc.argtypes = [vp, vp, vp, dp, dp, vp]
         L.smaug_get_state.argtypes = [vp, dp]
+        L.smaug_get_fields.argtypes = [vp, dp, ctypes.c_int32, ctypes.c_int32]
         L.smaug_set_state.argtypes = [vp, dp]
         L.smaug_get_time.argtypes = [vp, ctypes.POINTER(ctypes.c_int64), dp, dp]
         L.smaug_get_cmax.argtypes = [vp, dp]
@@ -173,6 +174,16 @@ class Engine:
         if w.shape != self.shape:
             raise ValueError("out has shape %s, expected %s" % (w.shape, self.shape))
         _check(lib().smaug_get_state(self.h, _dp(w)))
+        return w
+
+    def fields(self, f0, nf, out=None):
+        """Copy fields [f0, f0+nf) of the state to the host (into `out`, whose
+        leading dimension is nf, if given)."""
+        shape = (nf,) + self.shape[1:]
+        w = np.zeros(shape) if out is None else out
+        if w.shape != shape or not w.flags["C_CONTIGUOUS"]:
+            raise ValueError("out has shape %s, expected contiguous %s" % (w.shape, shape))
+        _check(lib().smaug_get_fields(self.h, _dp(w), int(f0), int(nf)))
         return w
 
     def set_state(self, w):

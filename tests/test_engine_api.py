@@ -13,7 +13,7 @@ pytestmark = pytest.mark.gpu
 
 def test_invalid_params_rejected(engine_lib):
     w, pos, dx = ot_rect(16, 16)
-    for kw, code in [({"integrator": 7}, 1), ({"pad_model": 9}, 1), ({"boundtype": (5, 0)}, 6),
+    for kw, code in [({"integrator": 7}, 1), ({"pad_model": 9}, 1), ({"boundtype": (1, 0)}, 6),
                      ({"gamma": 1.0}, 1)]:
         p = params_for(w, dx, **kw)
         with pytest.raises(engine_lib.SmaugError) as e:
@@ -122,3 +122,20 @@ def test_noalloc_rejects_3d(engine_lib):
     with pytest.raises(engine_lib.SmaugError) as e:
         engine_lib.euler_step_noalloc(p, 1, 2, d, 1e-3)
     assert e.value.code == 6
+
+
+def test_get_fields_subsets(engine_lib):
+    """smaug_get_fields: any contiguous range of fields equals the same rows of
+    smaug_get_state, across the evolved/background boundary too."""
+    w, pos, dx = ot_rect(24, 20, seed=3)
+    w[7] = 0.1
+    e = engine_lib.Engine(params_for(w, dx, integrator=P.INT_RK4), w, pos)
+    e.step(2)
+    full = e.state()
+    for f0, nf in [(0, 6), (0, 10), (3, 1), (5, 3), (6, 4), (9, 1)]:
+        got = e.fields(f0, nf)
+        assert np.array_equal(got, full[f0:f0 + nf]), (f0, nf)
+    with pytest.raises(engine_lib.SmaugError):
+        e.fields(8, 3)
+    e.close()
+
