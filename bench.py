@@ -414,6 +414,18 @@ def _adjoint_case(args, sa, q, p, u0, pos, rhob, theta0, shift, obs_z, nsteps, r
     return line
 
 
+def max_over_ranks(ms, ws, device="cuda"):
+    """The slowest rank's time: every rank takes part (the same collective in
+    the same order on every rank); one rank returns its own value."""
+    if ws <= 1:
+        return float(ms)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def dist_setup(args):
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -422,7 +434,8 @@ def dist_setup(args):
         import torch
         import torch.distributed as dist
         import datetime
-        torch.cuda.set_device(local)
+        if args.impl != "reference":  # the reference arm runs on the host cores only
+            torch.cuda.set_device(local)
         dist.init_process_group("nccl" if args.impl != "reference" else "gloo",
                                 timeout=datetime.timedelta(seconds=300))
     return ws, rank, local
@@ -582,11 +595,7 @@ def main():
     barrier()
     torch.cuda.synchronize()
     ms = ev0.elapsed_time(ev1)
-    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-    if ws > 1:
-        import torch.distributed as dist
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
+    ms_max = max_over_ranks(ms, ws)
     value = ncell_int * args.steps * ws / (ms_max / 1e3) / 1e6
     launches = 4 * args.steps
     ref_state = eng.state() if args.mixed else None
@@ -607,12 +616,7 @@ def main():
         eng.fields(0, nevo, out=host[:nevo])   # D2H of the step's result (the evolved fields)
     e1.record(stream)
     torch.cuda.synchronize()
-    e2e_ms = e0.elapsed_time(e1)
-    te = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
-    if ws > 1:
-        import torch.distributed as dist
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_ms = float(te.item())
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1), ws)
     e2e_val = ncell_int * args.e2e_steps * ws / (e2e_ms / 1e3) / 1e6
     h2d = (2 + 2 * p.ndim) * p.ncells * 8
     d2h = nevo * p.ncells * 8
@@ -640,12 +644,7 @@ def main():
         torch.cuda.synchronize()
         em.sync()
         barrier()
-        mms = m0.elapsed_time(m1)
-        tm = torch.tensor([mms], dtype=torch.float64, device="cuda")
-        if ws > 1:
-            import torch.distributed as dist
-            dist.all_reduce(tm, op=dist.ReduceOp.MAX)
-        mms = float(tm.item())
+        mms = max_over_ranks(m0.elapsed_time(m1), ws)
         mst = em.state()
         em.close()
         nevo = 2 + 2 * p.ndim
