@@ -15,6 +15,8 @@ model parameters with PGAMMA 1.66666667, courant 0.3, DT 1, moddton on):
   ot64     64x64 interior, 11 steps   -- multi-block (17 thread blocks)
   ot24x20  24x20 interior, steps 0-5  -- multi-block, consecutive steps for
            one-step parity away from the column the pad race can touch
+  ot128    128x128 interior, steps 1, 50, 200 -- the 128^2/200-step
+           configuration (34 blocks), run twice on the GPU box
 The reference launches one thread per cell in 512-thread blocks; its
 hyperdifvisc1r_parallel stores tmp6 through the wrong index (encode3) into
 the padded array while the same launch zeroes it.  Inside one block the
@@ -54,6 +56,8 @@ CASES = {
     "g18x12": (18, 12, 12, 21, [1, 2, 3, 5, 10, 20]),
     "ot64": (64, 64, 1, 12, [1, 11]),
     "ot24x20": (24, 20, 5, 12, [0, 1, 2, 3, 4, 5]),
+    # the small benchmark configuration: 128^2, 200 steps (34 thread blocks)
+    "ot128": (128, 128, 2, 201, [1, 50, 200]),
     # fixed (5) ghosts: the OT model's cuboundary (src/boundary.cu:231-252)
     # dispatches periodic only, so type 5 leaves the ghost layers as read
     # from the .ini; the gradient edge zeroing of non-periodic types applies
@@ -61,6 +65,7 @@ CASES = {
     "f18y": (18, 12, 14, 21, [1, 2, 3, 5, 10, 20], (0, 5)),
 }
 GAMMA_REF = 1.66666667  # models/iosmaugparams.h.ot PGAMMA
+TWICE = ("ot128",)      # run twice: the multi-block pad race makes runs differ
 
 # 3D: name: ((nx, ny, nz), seed, NT, steps kept, runs); runs > 1 repeats the
 # multi-block cases to expose order-dependent results
@@ -184,6 +189,8 @@ def _bc_defines(case):
 def run():
     for name, case in _selected(CASES).items():
         _run_one(name, case[4])
+        if name in TWICE:
+            _run_one(name, case[4], "_r1")
     for name, (n, seed, nt, keep, runs) in _selected(CASES3).items():
         for r in range(runs):
             _run_one(name, keep, "" if r == 0 else "_r%d" % r)
@@ -213,11 +220,16 @@ def collect():
             w, pos, h = formats.read_out(os.path.join(RUNS, name, "out", "ref_%d.out" % k))
             states.append(w[:6])
             times.append(h["t"])
+        extra = {}
+        # the last saved state of a second run of the same binary (name_r1)
+        if os.path.isdir(os.path.join(RUNS, name + "_r1")):
+            extra["last_r1"] = formats.read_out(
+                os.path.join(RUNS, name + "_r1", "out", "ref_%d.out" % keep[-1]))[0][:6]
         np.savez_compressed(os.path.join(HERE, name + ".npz"), w0=w0[:6], pos=pos0,
                             steps=np.array(keep), states=np.array(states),
                             hdr_t=np.array(times), gamma=GAMMA_REF,
                             dx=np.array([2 * math.pi / nx, 2 * math.pi / ny]),
-                            bt=np.array(bt))
+                            bt=np.array(bt), **extra)
         print("wrote", name)
 
 

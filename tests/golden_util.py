@@ -9,6 +9,7 @@ GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 STRICT = ("g16", "g18x12", "ot64")     # full multi-step runs
 BOUNDARY = ("f16x", "f18y")            # fixed ghosts along dim 0 / dim 1
 ONESTEP = ("ot24x20",)                 # consecutive steps, one-step parity
+RACE = ("ot128",)                      # 128^2, 200 steps, two runs of the reference
 STRICT3 = ("t3s", "t3a", "t3b")        # 3D flux-tube build, contcd4 ghosts, backgrounds
 
 
@@ -42,3 +43,14 @@ def full(w6):
     w = np.zeros((10,) + w6.shape[1:])
     w[:6] = w6
     return w
+
+
+def race_mask(d):
+    """Cells outside the last interior column along dim 0 and its periodic
+    image: the only cells the multi-block pad race of the reference reaches in
+    one step."""
+    n0 = d["w0"].shape[2]
+    mask = np.ones(d["w0"].shape[1:], bool)
+    mask[:, [1, n0 - 3]] = False
+    return mask
+

@@ -39,3 +39,34 @@ def test_engine_one_step_multiblock(engine_lib, name):
         e.close()
         for f in range(6):
             assert rel_l2(got[f][mask], d["states"][a + 1][f][mask]) <= TOL
+
+
+@pytest.mark.parametrize("name", G.RACE)
+def test_engine_first_step_outside_race_column(engine_lib, name):
+    d = G.load(name)
+    p = G.params(d)
+    e = engine_lib.Engine(p, d["w0full"], d["pos"])
+    e.step(1)
+    got = e.state()
+    e.close()
+    mask = G.race_mask(d)
+    for f in range(6):
+        assert rel_l2(got[f][mask], d["states"][0][f][mask]) <= TOL, f
+
+
+@pytest.mark.parametrize("name", G.RACE)
+def test_engine_200_steps_against_oracle(engine_lib, oracle, name):
+    """The engine and the oracle share the deterministic pad model; over 200
+    steps of the flow their rounding differences (~1e-16 per operation, sums
+    ordered differently) grow to ~1e-10, far below the reference's own
+    run-to-run spread (~3e-4) and below the stated 1e-8."""
+    d = G.load(name)
+    p = G.params(d)
+    e = engine_lib.Engine(p, d["w0full"], d["pos"])
+    e.step(200)
+    got = e.state()
+    e.close()
+    ref = oracle.OracleRun(p, d["w0full"], d["pos"]).advance(200)
+    errs = [rel_l2(got[f], ref.w[f]) for f in range(6)]
+    assert max(errs) <= 1e-8, errs
+
