@@ -201,36 +201,6 @@ __device__ __forceinline__ void ratio_bwd(const RInfo& r, double Rb, double* qvb
   qvb[r.f1] -= wb;
 }
 
-// q along direction D through a cell (region index l, coordinate a along D,
-// across coordinate tr), with the pads at coordinates -1 (copy of 5) and n
-// (stray-store source)
-template <int KIND, int COMP, int D>
-struct Line {
-  int l, a, n, tr;
-  static constexpr int SQ = D == 0 ? 1 : RX;
-  __device__ __forceinline__ double q(const A2& T, const AdjIn& I, long nc, int k) const {
-    const int ak = a + k;
-    if (ak == -1) return q_loc<KIND, COMP>(T, l + (k + 6) * SQ);
-    if (ak == n) {
-      const int src = I.padsrc[D][tr];
-      return src >= 0 ? q_glob<KIND, COMP>(I, nc, src) : 0.0;
-    }
-    return q_loc<KIND, COMP>(T, l + k * SQ);
-  }
-  __device__ __forceinline__ void qb(const A2& T, const AdjIn& I, long nc, int k, double v) const {
-    if (v == 0.0) return;
-    const int ak = a + k;
-    if (ak == -1) {
-      qbar_loc<KIND, COMP>(T, l + (k + 6) * SQ, v);
-    } else if (ak == n) {
-      const int src = I.padsrc[D][tr];
-      if (src >= 0) qbar_glob<KIND, COMP>(I, nc, src, v);
-    } else {
-      qbar_loc<KIND, COMP>(T, l + k * SQ, v);
-    }
-  }
-};
-
 // ---- flux Jacobian, transposed ----------------------------------------------
 // x = (rho, m1, m2, e, b1, b2) at one cell, g = (eb, rhob, bb1, bb2);
 // F = (F_rho, F_m1, F_m2, F_e, F_B across D) as in flux_at (stage2d.cuh);
@@ -360,140 +330,291 @@ __device__ __forceinline__ void cfast_vjp(double gamma, const double* x, const d
 }
 
 // ---- one hyperdiffusion pass, transposed ------------------------------------
-// Output cell i (region l, coordinates gi, gj, inside [2, n-3]); lam = k-bar
-// at i.  Mirrors hyper_pass of stage2d.cuh term by term.
+// Block-cooperative, in the phases of the forward pass (hyper_pass in
+// stage2d.cuh): (A) q of the pass on the staged region, (B) the nu ratio R with
+// its argmax faces on the ratio area, then the adjoint: (C) the cross-term
+// arrays at each nu-area cell j, gathered from the two tile cells whose
+// outputs difference them, and (D) the diagonal terms at each tile cell,
+// both accumulating R-bar (RB) and q-bar (QB); (E) R-bar through the argmax
+// faces into q-bar; (F) q-bar into the field adjoints, pads routed to their
+// sources.  All threads of the block call it.
+constexpr int ARSZ = (TX + 1) * (TY + 2) > (TX + 2) * (TY + 1) ? (TX + 1) * (TY + 2) : (TX + 2) * (TY + 1);
+
+struct PassScratch {
+  double* Q;    // [RC] q of the pass (pads included)
+  double* QB;   // [RC] q-bar
+  double* RR;   // [ARSZ] ratio R
+  double* T5;   // [ARSZ] its denominator max D1
+  double* RB;   // [ARSZ] R-bar
+  int* code;    // [ARSZ] argmax faces and signs
+};
+
+__device__ __forceinline__ int pack_code(const RInfo& r) {
+  return r.f3 | (r.f1 << 2) | ((r.s3 > 0) << 5) | ((r.s1 > 0) << 6);
+}
+__device__ __forceinline__ RInfo unpack(double R, double T5, int c) {
+  RInfo r;
+  r.R = R;
+  r.T5 = T5;
+  r.T4 = R * T5;  // only its sign is used (R > 0 iff T4 > 0 where T5 > 0)
+  r.f3 = c & 3;
+  r.f1 = (c >> 2) & 7;
+  r.s3 = (c & 32) ? 1.0 : -1.0;
+  r.s1 = (c & 64) ? 1.0 : -1.0;
+  return r;
+}
+
+// (A) q of the pass field on the region with the reference's pads; q-bar
+// cleared.  The passes of both directions of one field share q and q-bar; the
+// caller places the barrier (the next field's staging runs beside the
+// previous field's flush, on the other q-bar buffer).
+template <int KIND, int COMP>
+__device__ __forceinline__ void adj_stage_q(const A2& T, const AdjIn& I, const KParams& P,
+                                            const PassScratch& W, int tid) {
+  const long nc = P.ncell;
+  const int n0 = P.n0, n1 = P.n1;
+  // (A) q on the region with the reference's pads; q-bar cleared
+  for (int r = tid; r < RC; r += ANT) {
+    const int lx = r % RX, ly = r / RX;
+    const int ci = T.x0 - HALO + lx, cj = T.y0 - HALO + ly;
+    const bool inx = ci >= 0 && ci < n0, iny = cj >= 0 && cj < n1;
+    double q = 0.0;
+    if (inx && iny) {
+      q = q_loc<KIND, COMP>(T, r);
+    } else if (iny) {
+      if (ci == -1) {
+        q = q_loc<KIND, COMP>(T, r + 6);
+      } else if (ci == n0) {
+        const int src = I.padsrc[0][cj];
+        if (src >= 0) q = q_glob<KIND, COMP>(I, nc, src);
+      }
+    } else if (inx) {
+      if (cj == -1) {
+        q = q_loc<KIND, COMP>(T, r + 6 * RX);
+      } else if (cj == n1) {
+        const int src = I.padsrc[1][ci];
+        if (src >= 0) q = q_glob<KIND, COMP>(I, nc, src);
+      }
+    }
+    W.Q[r] = q;
+    W.QB[r] = 0.0;
+  }
+}
+
+// (B)-(E) of one pass on the staged q: R-bar and q-bar accumulated
 template <int KIND, int COMP, int DIM>
-__device__ __forceinline__ void hyp_adj(const A2& T, const AdjIn& I, const KParams& P, int lxo, int lyo,
-                                        int gi, int gj, const double* lam, double* sb) {
+__device__ __forceinline__ void hyp_pass_adj(const A2& T, const AdjIn& I, const KParams& P,
+                                             const PassScratch& W, int tid, bool active, int lxo,
+                                             int lyo, int gi, int gj, const double* Lam, double* sb) {
   constexpr bool CROSS = (KIND == 2 && COMP != DIM) || (KIND == 3);
   constexpr int QF = (KIND == 0) ? RHO : (KIND == 1) ? EN : (KIND == 2) ? M1 + COMP : B1 + COMP;
-  constexpr int SL = DIM == 0 ? 1 : RX;
-  const long nc = P.ncell;
+  constexpr int SQ = DIM == 0 ? 1 : RX;  // stride along DIM in the region
+  constexpr int SL = SQ;
+  // ratio area: the tile along DIM extended by one cell below, +-1 across
+  // when cross terms need it (as the forward)
+  constexpr int exR = DIM == 0 ? TX + 1 : (CROSS ? TX + 2 : TX);
+  constexpr int eyR = DIM == 0 ? (CROSS ? TY + 2 : TY) : TY + 1;
+  constexpr int oxR = DIM == 0 ? HALO - 1 : (CROSS ? HALO - 1 : HALO);
+  constexpr int oyR = DIM == 0 ? (CROSS ? HALO - 1 : HALO) : HALO - 1;
+  constexpr int SR = DIM == 0 ? 1 : exR;  // stride along DIM in the ratio area
+  // nu area: the tile along DIM, +-1 across
+  constexpr int exN = DIM == 0 ? TX : TX + 2, eyN = DIM == 0 ? TY + 2 : TY;
+  constexpr int oxN = DIM == 0 ? HALO : HALO - 1, oyN = DIM == 0 ? HALO - 1 : HALO;
   const int n0 = P.n0, n1 = P.n1, nd = DIM == 0 ? n0 : n1;
   const double dt = I.dt;
   const double chyp = P.chyp[QF], coef = I.cmax[DIM] * chyp;
-  const int l = lyo * RX + lxo;
-  const int a = DIM == 0 ? gi : gj;
-  const Line<KIND, COMP, DIM> L{l, a, nd, DIM == 0 ? gj : gi};
-  double qs[7];
-#pragma unroll
-  for (int k = 0; k < 7; k++) qs[k] = L.q(T, I, nc, k - 3);
-  const RInfo Ri = ratio_of(qs + 1), Rm = ratio_of(qs);  // R(i), R(i-1)
-  const double dl = DIM == 0 ? T.dl0[lxo] : T.dl1[lyo];
-  const double rdl = DIM == 0 ? T.rd0[lxo] : T.rd1[lyo];
-  const double c = dl * coef;
-  const double nur = c * Ri.R, nul = c * Rm.R;
-  const double qc = qs[3], qp = qs[4], qm = qs[2];
-  const bool z = (P.bt[DIM] != 0) && zero1n(a, nd);
-  const double gr = z ? 0.0 : (qp - qc) * rdl, gl = z ? 0.0 : (qc - qm) * rdl;
-  double qsb[7] = {0, 0, 0, 0, 0, 0, 0};
-  double nurb = 0, nulb = 0, grb = 0, glb = 0;
-  if (KIND == 0 || KIND == 1) {
-    const double ab = lam[QF] * dt * rdl;
-    nurb += ab * gr;
-    nulb -= ab * gl;
-    grb += ab * nur;
-    glb -= ab * nul;
-  } else if (KIND == 2) {
-    const double mult = (COMP == DIM) ? 2.0 : 1.0;
-    const double r0 = T.v(RHO, l) + T.v(RHOB, l);
-    const double t2 = (r0 + T.v(RHO, l - SL) + T.v(RHOB, l - SL)) * 0.5;
-    const double t3 = (r0 + T.v(RHO, l + SL) + T.v(RHOB, l + SL)) * 0.5;
-    const double mf = T.v(M1 + COMP, l);
-    const double t5 = (mf + T.v(M1 + COMP, l - SL)) * 0.5;
-    const double t6 = (mf + T.v(M1 + COMP, l + SL)) * 0.5;
-    const double am = lam[M1 + COMP] * dt * mult * rdl * 0.5;
-    const double ae = lam[EN] * dt * mult * rdl * 0.5;
-    const double t3b = am * nur * gr, t2b = -am * nul * gl;
-    const double t6b = ae * nur * gr, t5b = -ae * nul * gl;
-    nurb += am * t3 * gr + ae * t6 * gr;
-    grb += am * t3 * nur + ae * t6 * nur;
-    nulb -= am * t2 * gl + ae * t5 * gl;
-    glb -= am * t2 * nul + ae * t5 * nul;
-    sadd(T.A + RHO * RC + l, 0.5 * (t2b + t3b));
-    sadd(T.A + RHO * RC + l - SL, 0.5 * t2b);
-    sadd(T.A + RHO * RC + l + SL, 0.5 * t3b);
-    sadd(T.A + (M1 + COMP) * RC + l, 0.5 * (t5b + t6b));
-    sadd(T.A + (M1 + COMP) * RC + l - SL, 0.5 * t5b);
-    sadd(T.A + (M1 + COMP) * RC + l + SL, 0.5 * t6b);
-  } else {
-    // diagonal B term (hyperdifbsource, sb = +1), q = B_COMP
-    const double aB = lam[B1 + COMP] * dt * rdl;
-    const double ae = lam[EN] * dt * rdl;
-    const double t2 = (qc + qm) * 0.5, t3 = (qc + qp) * 0.5;
-    grb += aB * nur + ae * t3 * nur;
-    nurb += aB * gr + ae * t3 * gr;
-    glb -= aB * nul + ae * t2 * nul;
-    nulb -= aB * gl + ae * t2 * gl;
-    const double t3b = ae * gr * nur, t2b = -ae * gl * nul;
-    qsb[3] += 0.5 * (t2b + t3b);
-    qsb[2] += 0.5 * t2b;
-    qsb[4] += 0.5 * t3b;
-  }
-  if (!z) {
-    qsb[4] += grb * rdl;
-    qsb[3] -= grb * rdl;
-    qsb[3] += glb * rdl;
-    qsb[2] -= glb * rdl;
-  }
-  sb[DIM] += nurb * dl * chyp * Ri.R + nulb * dl * chyp * Rm.R;
-  ratio_bwd(Ri, nurb * c, qsb + 1);
-  ratio_bwd(Rm, nulb * c, qsb);
-#pragma unroll
-  for (int k = 0; k < 7; k++) L.qb(T, I, nc, k - 3, qsb[k]);
+  auto ri = [&](int lx, int ly) { return (ly - oyR) * exR + (lx - oxR); };
 
+  // (B) R = max D3(i-1..i+1) / max D1(i-2..i+2) and its argmax faces
+  for (int r = tid; r < exR * eyR; r += ANT) {
+    const int lx = oxR + r % exR, ly = oyR + r / exR;
+    const int l = ly * RX + lx;
+    double qv[6];
+#pragma unroll
+    for (int k = 0; k < 6; k++) qv[k] = W.Q[l + (k - 2) * SQ];
+    const RInfo Ri = ratio_of(qv);
+    W.RR[r] = Ri.R;
+    W.T5[r] = Ri.T5;
+    W.code[r] = pack_code(Ri);
+    W.RB[r] = 0.0;
+  }
+  __syncthreads();
+  // (C) cross terms: d/dx_COMP of C3 = rho_t tau, C4 = tau m_DIM (momentum) or
+  // C3 = t3, C4 = t3 B_DIM (field; the outputs take them with a minus sign),
+  // tau = g nsum / 4, t3 = g nsum / 2, at the nu-area cells j
   if (CROSS) {
-    // cross terms: d/dx_COMP of C3 = rho_t tau, C4 = tau m_DIM (momentum) or
-    // C3 = t3, C4 = t3 B_DIM (field, with the minus sign of sb = -1), with
-    // tau = g (nu_r + nu_l)/4, t3 = g (nu_r + nu_l)/2 at j = i +- e_COMP
-    constexpr int SC = COMP == 0 ? 1 : RX;
-    const int af = COMP == 0 ? gi : gj;
-    const int nf = COMP == 0 ? n0 : n1;
-    if ((P.bt[COMP] != 0) && zero1n(af, nf)) return;
-    const double rdf = COMP == 0 ? T.rd0[lxo] : T.rd1[lyo];
-    const double sgn = (KIND == 2) ? 1.0 : -1.0;
-    const double lx_ = (KIND == 2) ? lam[M1 + DIM] : lam[B1 + DIM];
+    for (int r = tid; r < exN * eyN; r += ANT) {
+      const int lx = oxN + r % exN, ly = oyN + r / exN;
+      const int jx = T.x0 - HALO + lx, jy = T.y0 - HALO + ly;
+      if (!(jx >= 2 && jx <= n0 - 3 && jy >= 2 && jy <= n1 - 3)) continue;  // nsum = 0 there
+      // C3-bar, C4-bar from the tile cells i = j -+ e_COMP
+      double C3b = 0.0, C4b = 0.0;
 #pragma unroll
-    for (int s = -1; s <= 1; s += 2) {
-      const int jx = gi + (COMP == 0 ? s : 0), jy = gj + (COMP == 1 ? s : 0);
-      if (!(jx >= 2 && jx <= n0 - 3 && jy >= 2 && jy <= n1 - 3)) continue;  // nu = 0 there
-      const int lj = l + s * SC;
-      const double C3b = sgn * s * lx_ * dt * rdf * 0.5;
-      const double C4b = sgn * s * lam[EN] * dt * rdf * 0.5;
-      const Line<KIND, COMP, DIM> Lj{lj, a, nd, DIM == 0 ? jy : jx};
-      double qj[7];
-#pragma unroll
-      for (int k = 0; k < 7; k++) qj[k] = Lj.q(T, I, nc, k - 3);
-      const RInfo Rj = ratio_of(qj + 1), Rjm = ratio_of(qj);
-      const double nsum = c * Rj.R + c * Rjm.R;
+      for (int s = -1; s <= 1; s += 2) {
+        const int ix = lx - HALO - (COMP == 0 ? s : 0), iy = ly - HALO - (COMP == 1 ? s : 0);
+        if (ix < 0 || ix >= TX || iy < 0 || iy >= TY) continue;
+        const int ci = T.x0 + ix, cj = T.y0 + iy;
+        if (!(ci <= n0 - 3 && cj <= n1 - 3)) continue;  // not an output cell
+        const int af = COMP == 0 ? ci : cj;
+        if ((P.bt[COMP] != 0) && zero1n(af, COMP == 0 ? n0 : n1)) continue;
+        const int it = iy * TX + ix;
+        const double rdf = COMP == 0 ? T.rd0[ix + HALO] : T.rd1[iy + HALO];
+        const double sgn = (KIND == 2) ? 1.0 : -1.0;
+        const double lx_ = (KIND == 2) ? Lam[(M1 + DIM) * ANT + it] : Lam[(B1 + DIM) * ANT + it];
+        C3b += sgn * s * lx_ * dt * rdf * 0.5;
+        C4b += sgn * s * Lam[EN * ANT + it] * dt * rdf * 0.5;
+      }
+      if (C3b == 0.0 && C4b == 0.0) continue;
+      const int l = ly * RX + lx;
+      const int a = DIM == 0 ? jx : jy;
+      const double dl = DIM == 0 ? T.dl0[lx] : T.dl1[ly];
+      const double rdl = DIM == 0 ? T.rd0[lx] : T.rd1[ly];
+      const double c = dl * coef;
+      const int rr = ri(lx, ly);
+      const double Rj = W.RR[rr], Rjm = W.RR[rr - SR];
+      const double nsum = c * Rj + c * Rjm;
       const bool zj = (P.bt[DIM] != 0) && zero1n(a, nd);
-      const double g = zj ? 0.0 : ((qj[4] - qj[2]) * rdl) * 0.5;
+      const double g = zj ? 0.0 : ((W.Q[l + SQ] - W.Q[l - SQ]) * rdl) * 0.5;
       double tb;
       if (KIND == 2) {
         const double tau = (g * nsum) * 0.25;
-        const double rtj = T.v(RHO, lj) + T.v(RHOB, lj), mdj = T.v(M1 + DIM, lj);
-        tb = C3b * rtj + C4b * mdj;
-        sadd(T.A + RHO * RC + lj, C3b * tau);
-        sadd(T.A + (M1 + DIM) * RC + lj, C4b * tau);
+        tb = C3b * (T.v(RHO, l) + T.v(RHOB, l)) + C4b * T.v(M1 + DIM, l);
+        sadd(T.A + RHO * RC + l, C3b * tau);
+        sadd(T.A + (M1 + DIM) * RC + l, C4b * tau);
         tb *= 0.25;
       } else {
         const double t3 = (g * nsum) * 0.5;
-        const double bdj = T.v(B1 + DIM, lj);
-        tb = C3b + C4b * bdj;
-        sadd(T.A + (B1 + DIM) * RC + lj, C4b * t3);
+        tb = C3b + C4b * T.v(B1 + DIM, l);
+        sadd(T.A + (B1 + DIM) * RC + l, C4b * t3);
         tb *= 0.5;
       }
       const double gb = tb * nsum, nsb = tb * g;
-      double qjb[7] = {0, 0, 0, 0, 0, 0, 0};
       if (!zj) {
-        qjb[4] += gb * rdl * 0.5;
-        qjb[2] -= gb * rdl * 0.5;
+        sadd(W.QB + l + SQ, gb * rdl * 0.5);
+        sadd(W.QB + l - SQ, -gb * rdl * 0.5);
       }
-      sb[DIM] += nsb * dl * chyp * (Rj.R + Rjm.R);
-      ratio_bwd(Rj, nsb * c, qjb + 1);
-      ratio_bwd(Rjm, nsb * c, qjb);
+      sb[DIM] += nsb * dl * chyp * (Rj + Rjm);
+      sadd(W.RB + rr, nsb * c);
+      sadd(W.RB + rr - SR, nsb * c);
+    }
+  }
+  // (D) the diagonal terms at the tile cells
+  if (active) {
+    const int l = lyo * RX + lxo;
+    const int a = DIM == 0 ? gi : gj;
+    const double dl = DIM == 0 ? T.dl0[lxo] : T.dl1[lyo];
+    const double rdl = DIM == 0 ? T.rd0[lxo] : T.rd1[lyo];
+    const double c = dl * coef;
+    const int rr = ri(lxo, lyo);
+    const double Ri = W.RR[rr], Rm = W.RR[rr - SR];
+    const double nur = c * Ri, nul = c * Rm;
+    const double qc = W.Q[l], qp = W.Q[l + SQ], qm = W.Q[l - SQ];
+    const bool z = (P.bt[DIM] != 0) && zero1n(a, nd);
+    const double gr = z ? 0.0 : (qp - qc) * rdl, gl = z ? 0.0 : (qc - qm) * rdl;
+    const int tid_ = tid;
+    auto lam = [&](int f) { return Lam[f * ANT + tid_]; };
+    double nurb = 0, nulb = 0, grb = 0, glb = 0;
+    double qb0 = 0, qbm = 0, qbp = 0;  // q-bar at i, i-1, i+1
+    if (KIND == 0 || KIND == 1) {
+      const double ab = lam(QF) * dt * rdl;
+      nurb += ab * gr;
+      nulb -= ab * gl;
+      grb += ab * nur;
+      glb -= ab * nul;
+    } else if (KIND == 2) {
+      const double mult = (COMP == DIM) ? 2.0 : 1.0;
+      const double r0 = T.v(RHO, l) + T.v(RHOB, l);
+      const double t2 = (r0 + T.v(RHO, l - SL) + T.v(RHOB, l - SL)) * 0.5;
+      const double t3 = (r0 + T.v(RHO, l + SL) + T.v(RHOB, l + SL)) * 0.5;
+      const double mf = T.v(M1 + COMP, l);
+      const double t5 = (mf + T.v(M1 + COMP, l - SL)) * 0.5;
+      const double t6 = (mf + T.v(M1 + COMP, l + SL)) * 0.5;
+      const double am = lam(M1 + COMP) * dt * mult * rdl * 0.5;
+      const double ae = lam(EN) * dt * mult * rdl * 0.5;
+      const double t3b = am * nur * gr, t2b = -am * nul * gl;
+      const double t6b = ae * nur * gr, t5b = -ae * nul * gl;
+      nurb += am * t3 * gr + ae * t6 * gr;
+      grb += am * t3 * nur + ae * t6 * nur;
+      nulb -= am * t2 * gl + ae * t5 * gl;
+      glb -= am * t2 * nul + ae * t5 * nul;
+      sadd(T.A + RHO * RC + l, 0.5 * (t2b + t3b));
+      sadd(T.A + RHO * RC + l - SL, 0.5 * t2b);
+      sadd(T.A + RHO * RC + l + SL, 0.5 * t3b);
+      sadd(T.A + (M1 + COMP) * RC + l, 0.5 * (t5b + t6b));
+      sadd(T.A + (M1 + COMP) * RC + l - SL, 0.5 * t5b);
+      sadd(T.A + (M1 + COMP) * RC + l + SL, 0.5 * t6b);
+    } else {
+      // diagonal B term (hyperdifbsource, sb = +1), q = B_COMP
+      const double aB = lam(B1 + COMP) * dt * rdl;
+      const double ae = lam(EN) * dt * rdl;
+      const double t2 = (qc + qm) * 0.5, t3 = (qc + qp) * 0.5;
+      grb += aB * nur + ae * t3 * nur;
+      nurb += aB * gr + ae * t3 * gr;
+      glb -= aB * nul + ae * t2 * nul;
+      nulb -= aB * gl + ae * t2 * gl;
+      const double t3b = ae * gr * nur, t2b = -ae * gl * nul;
+      qb0 += 0.5 * (t2b + t3b);
+      qbm += 0.5 * t2b;
+      qbp += 0.5 * t3b;
+    }
+    if (!z) {
+      qbp += grb * rdl;
+      qb0 -= grb * rdl;
+      qb0 += glb * rdl;
+      qbm -= glb * rdl;
+    }
+    sadd(W.QB + l, qb0);
+    sadd(W.QB + l - SQ, qbm);
+    sadd(W.QB + l + SQ, qbp);
+    sb[DIM] += nurb * dl * chyp * Ri + nulb * dl * chyp * Rm;
+    sadd(W.RB + rr, nurb * c);
+    sadd(W.RB + rr - SR, nulb * c);
+  }
+  __syncthreads();
+  // (E) R-bar through the argmax faces into q-bar
+  for (int r = tid; r < exR * eyR; r += ANT) {
+    const double Rb = W.RB[r];
+    if (Rb == 0.0) continue;
+    const int lx = oxR + r % exR, ly = oyR + r / exR;
+    const int l = ly * RX + lx;
+    const RInfo Ri = unpack(W.RR[r], W.T5[r], W.code[r]);
+    double qvb[6] = {0, 0, 0, 0, 0, 0};
+    ratio_bwd(Ri, Rb, qvb);
 #pragma unroll
-      for (int k = 0; k < 7; k++) Lj.qb(T, I, nc, k - 3, qjb[k]);
+    for (int k = 0; k < 6; k++) sadd(W.QB + l + (k - 2) * SQ, qvb[k]);
+  }
+  __syncthreads();
+}
+
+// (F) q-bar of the field into the field adjoints; pads routed to the cells
+// they copy (the caller places the barrier)
+template <int KIND, int COMP>
+__device__ __forceinline__ void adj_flush_q(const A2& T, const AdjIn& I, const KParams& P,
+                                            const PassScratch& W, int tid) {
+  const long nc = P.ncell;
+  const int n0 = P.n0, n1 = P.n1;
+  for (int r = tid; r < RC; r += ANT) {
+    const double qb = W.QB[r];
+    if (qb == 0.0) continue;
+    const int lx = r % RX, ly = r / RX;
+    const int ci = T.x0 - HALO + lx, cj = T.y0 - HALO + ly;
+    const bool inx = ci >= 0 && ci < n0, iny = cj >= 0 && cj < n1;
+    if (inx && iny) {
+      qbar_loc<KIND, COMP>(T, r, qb);
+    } else if (iny) {
+      if (ci == -1) {
+        qbar_loc<KIND, COMP>(T, r + 6, qb);
+      } else if (ci == n0) {
+        const int src = I.padsrc[0][cj];
+        if (src >= 0) qbar_glob<KIND, COMP>(I, nc, src, qb);
+      }
+    } else if (inx) {
+      if (cj == -1) {
+        qbar_loc<KIND, COMP>(T, r + 6 * RX, qb);
+      } else if (cj == n1) {
+        const int src = I.padsrc[1][ci];
+        if (src >= 0) qbar_glob<KIND, COMP>(I, nc, src, qb);
+      }
     }
   }
 }
@@ -635,22 +756,49 @@ __global__ void __launch_bounds__(ANT, SMAUG_ADJ_MINB) adj_stage2d(const KParams
   }
   __syncthreads();
 
-  // ---- hyperdiffusion and driver (scatter per output cell) ----------------
+  // ---- hyperdiffusion (block-cooperative passes) and driver ---------------
   double sb[2] = {0, 0}, th[3] = {0, 0, 0};
   const int lxo = tx + HALO, lyo = ty + HALO, lo = lyo * RX + lxo;
+  if (P.hyperdif == 1) {
+    // the passes grouped by field (their contributions add up, in any order)
+    PassScratch Wa, Wb;
+    Wa.Q = T.rd1 + RY;
+    Wa.QB = Wa.Q + RC;
+    Wa.RR = Wa.QB + 2 * RC;
+    Wa.T5 = Wa.RR + ARSZ;
+    Wa.RB = Wa.T5 + ARSZ;
+    Wa.code = reinterpret_cast<int*>(Wa.RB + ARSZ);
+    Wb = Wa;
+    Wb.QB = Wa.QB + RC;
+#define HPA(W, K, C, D) hyp_pass_adj<K, C, D>(T, I, P, W, tid, active, lxo, lyo, gi, gj, Lam, sb)
+    adj_stage_q<0, 0>(T, I, P, Wa, tid);
+    __syncthreads();
+    HPA(Wa, 0, 0, 0); HPA(Wa, 0, 0, 1);
+    adj_flush_q<0, 0>(T, I, P, Wa, tid);
+    adj_stage_q<1, 0>(T, I, P, Wb, tid);
+    __syncthreads();
+    HPA(Wb, 1, 0, 0); HPA(Wb, 1, 0, 1);
+    adj_flush_q<1, 0>(T, I, P, Wb, tid);
+    adj_stage_q<2, 0>(T, I, P, Wa, tid);
+    __syncthreads();
+    HPA(Wa, 2, 0, 0); HPA(Wa, 2, 0, 1);
+    adj_flush_q<2, 0>(T, I, P, Wa, tid);
+    adj_stage_q<2, 1>(T, I, P, Wb, tid);
+    __syncthreads();
+    HPA(Wb, 2, 1, 0); HPA(Wb, 2, 1, 1);
+    adj_flush_q<2, 1>(T, I, P, Wb, tid);
+    adj_stage_q<3, 1>(T, I, P, Wa, tid);
+    __syncthreads();
+    HPA(Wa, 3, 1, 0);
+    adj_flush_q<3, 1>(T, I, P, Wa, tid);
+    adj_stage_q<3, 0>(T, I, P, Wb, tid);
+    __syncthreads();
+    HPA(Wb, 3, 0, 1);
+    adj_flush_q<3, 0>(T, I, P, Wb, tid);
+    __syncthreads();
+#undef HPA
+  }
   if (active) {
-    if (P.hyperdif == 1) {
-      hyp_adj<0, 0, 0>(T, I, P, lxo, lyo, gi, gj, lam, sb);
-      hyp_adj<0, 0, 1>(T, I, P, lxo, lyo, gi, gj, lam, sb);
-      hyp_adj<1, 0, 0>(T, I, P, lxo, lyo, gi, gj, lam, sb);
-      hyp_adj<1, 0, 1>(T, I, P, lxo, lyo, gi, gj, lam, sb);
-      hyp_adj<2, 0, 0>(T, I, P, lxo, lyo, gi, gj, lam, sb);
-      hyp_adj<2, 1, 0>(T, I, P, lxo, lyo, gi, gj, lam, sb);
-      hyp_adj<2, 0, 1>(T, I, P, lxo, lyo, gi, gj, lam, sb);
-      hyp_adj<2, 1, 1>(T, I, P, lxo, lyo, gi, gj, lam, sb);
-      hyp_adj<3, 1, 0>(T, I, P, lxo, lyo, gi, gj, lam, sb);
-      hyp_adj<3, 0, 1>(T, I, P, lxo, lyo, gi, gj, lam, sb);
-    }
     if (P.driver == SMAUG_DRIVER_GAUSS) {
       // m_1 += dt v (rho + rho_b), v = amp sin(2 pi t/P) prod_d exp(-(x_d-x0_d)^2/s_d^2)
       const double tt = I.tstage;
@@ -904,7 +1052,10 @@ static void free_adj(Adjoint* a) {
   delete a;
 }
 
-static size_t adj_smem() { return sizeof(double) * ((size_t)17 * RC + 6 * ANT + 2 * (RX + RY)); }
+static size_t adj_smem() {
+  return sizeof(double) * ((size_t)17 * RC + 6 * ANT + 2 * (RX + RY) + 3 * RC + 3 * ARSZ) +
+         sizeof(int) * ARSZ;
+}
 
 static int adj_create(const smaug_params_t* p, const double* w, const double* pos, Adjoint** out) {
   if (!p || !w || !pos || !out) return set_error(SMAUG_E_INVALID, "null argument");
