@@ -189,3 +189,56 @@ def test_reference_driver_on_engine_mixed(tmp_path):
     errs = [_rel(w[f], ref[f]) for f in range(6)]
     assert max(errs) <= 1e-4, errs
     assert max(errs) > 0.0  # the float stage buffers were used
+
+
+SHIM_PROBE = r"""
+#include <cstdio>
+#include <cstring>
+#include <vector>
+#include "smaug_compat.h"
+int main(int argc, char** argv) {
+  params* p = new params();
+  std::memset(p, 0, sizeof(params));
+  p->n[0] = 12; p->n[1] = 12;
+  p->rkon = argv[1][0] == 'r' ? 1 : 0;
+  for (int f = 0; f < SMAUG_COMPAT_NVAR; f++)
+    for (int d = 0; d < SMAUG_COMPAT_NDIM; d++) p->boundtype[f][d][0] = p->boundtype[f][d][1] = 0;
+  if (argv[1][0] == 'b') p->boundtype[0][1][0] = 7;
+  state* st = new state();
+  bparams* bp = nullptr;
+  std::vector<double> wmod(2 * SMAUG_COMPAT_NVAR * 144), wd(19 * 144);
+  double *w = wmod.data(), *wdp = wd.data(), *dummy = nullptr;
+  params* dp = nullptr; bparams* dbp = nullptr; state* ds = nullptr;
+  cuinit(&p, &bp, &w, &dummy, &wdp, &st, &dp, &dbp, &dummy, &dummy, &dummy, &dummy, &ds, &dummy,
+         &dummy, &dummy);
+  std::printf("cuinit returned\n");
+  std::fflush(stdout);
+  cuboundary(&p, &bp, &dp, &dbp, &ds, &dummy, 0, 1, 0);
+  std::printf("cuboundary returned\n");
+  return 0;
+}
+"""
+
+
+@pytest.mark.parametrize("mode,expect_rc,needle", [
+    ("ok", 0, None),
+    ("rk", 3, "rkon=1"),
+    ("bc", 3, "boundary type"),
+])
+def test_shim_refuses_unsupported_driver_use(engine_lib, tmp_path, mode, expect_rc, needle):
+    """The reference's driver ignores wrapper return values, so the shim ends
+    the process (status 3, message on stderr) on a use it does not support:
+    the RK driver, or a boundary type other than 0/4/5.  (No device work is
+    reached: the engine is created at the first step.)"""
+    src = tmp_path / "probe.cpp"
+    src.write_text(SHIM_PROBE)
+    exe = tmp_path / "probe"
+    subprocess.check_call(["g++", "-DUSE_SAC", "-I", os.path.join(ROOT, "include"), str(src), "-o",
+                           str(exe), "-L", PKG, "-lsmaug_compat2d", "-lsmaug_b200",
+                           "-Wl,-rpath," + PKG])
+    r = subprocess.run([str(exe), mode], capture_output=True, text=True, timeout=60)
+    assert r.returncode == expect_rc, (r.returncode, r.stdout, r.stderr)
+    if needle:
+        assert "smaug_compat:" in r.stderr and needle in r.stderr, r.stderr
+    else:
+        assert "cuboundary returned" in r.stdout
