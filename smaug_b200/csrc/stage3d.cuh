@@ -33,7 +33,19 @@
 
 // (included inside namespace smaug)
 namespace s3 {
-constexpr int T0 = 8, T1 = 8, T2 = 4;  // tile (x fastest)
+#ifndef SMAUG_T3X
+#define SMAUG_T3X 8
+#endif
+#ifndef SMAUG_T3Y
+#define SMAUG_T3Y 8
+#endif
+#ifndef SMAUG_T3Z
+#define SMAUG_T3Z 4
+#endif
+#ifndef SMAUG_MINB3D
+#define SMAUG_MINB3D 3  // resident blocks per SM the 3D stage is compiled for
+#endif
+constexpr int T0 = SMAUG_T3X, T1 = SMAUG_T3Y, T2 = SMAUG_T3Z;  // tile (x fastest)
 constexpr int NT = T0 * T1 * T2;       // threads per block, one cell each
 constexpr int H = 3;                   // box halo
 constexpr int BX = T0 + 2 * H, BY = T1 + 2 * H, BZ = T2 + 2 * H;
@@ -418,7 +430,7 @@ __device__ __forceinline__ void flux_pass3(const Box3& X, const KParams& P, cons
 }
 
 template <int MODE, bool BG, bool MIX>
-__global__ void __launch_bounds__(s3::NT, 3) stage3d_fast(const KParams P, const KBufs B) {
+__global__ void __launch_bounds__(s3::NT, SMAUG_MINB3D) stage3d_fast(const KParams P, const KBufs B) {
   using ST = typename Form<MIX>::S;
   const ST* u = static_cast<const ST*>(B.uin);
   extern __shared__ double smem[];
