@@ -31,6 +31,15 @@ def ensemble(precision):
     p, w, pos = slab(48, 64, 30.0, 5)
     p.precision = precision
     runs.append((p, w, pos))
+    # fixed and antisymmetric ghosts in the same launch
+    w, pos, dx = ot_rect(40, 36, seed=6)
+    runs.append((params_for(w, dx, integrator=P.INT_RK4, precision=precision,
+                            boundtype=(P.BC_FIXED, P.BC_PERIODIC)), w, pos))
+    w, pos, dx = ot_rect(34, 30, seed=7)
+    w[:6] *= 0.01
+    w[6], w[7], w[8], w[9] = 2.0, 1.0, 0.1, 0.05
+    runs.append((params_for(w, dx, integrator=P.INT_RK4, precision=precision,
+                            boundtype=(P.BC_ASYMM, P.BC_CONTCD4)), w, pos))
     return runs
 
 
