@@ -75,6 +75,10 @@ CASES3 = {
     "t3s": ((4, 4, 4), 21, 21, [1, 2, 3, 5, 10, 20], 1),
     "t3a": ((12, 12, 8), 22, 12, [0, 1, 2, 3, 4, 5, 10], 2),
     "t3b": ((20, 12, 8), 23, 5, [0, 1, 2, 3], 2),
+    # fixed ghosts along dim 0: the flux-tube model's cuboundary leaves type 3
+    # untouched at run time (models/boundary.cu.fluxtube1:1137-1277), which
+    # is the engine's fixed type (5)
+    "t3f": ((4, 4, 4), 24, 21, [1, 2, 3, 5, 10, 20], 1, (3, 4, 4), (5, 4, 4)),
 }
 
 
@@ -113,12 +117,16 @@ def tube_state(nx, ny, nz, seed, gamma=GAMMA_REF):
     return w, np.stack([X, Y, Z])
 
 
-def _build3(name, nx, ny, nz, nt):
+def _build3(name, nx, ny, nz, nt, bt_ref=None):
     from oracle import build_ref
+    extra = {}
+    for d, t in enumerate(bt_ref or ()):
+        extra["BCU%d" % d] = str(t)
+        extra["BCL%d" % d] = str(t)
     return build_ref.build_ref(name, nx, ny, nt, nk=nz, verbose=False,
                                XMIN="0.0", XMAX=repr(L3), YMIN="0.0", YMAX=repr(L3),
                                ZMIN="0.0", ZMAX=repr(L3), PGRAV0=repr(G3), PGRAV1="0.0",
-                               PGRAV2="0.0")
+                               PGRAV2="0.0", **extra)
 
 
 def _selected(table):
@@ -154,11 +162,12 @@ def prepare():
         formats.write_ini(os.path.join(WORK, name + ".ini"), w, pos)
         build_ref.build_ref(name, nx, ny, nt, verbose=False, **_bc_defines(case))
         print("prepared", name)
-    for name, ((nx, ny, nz), seed, nt, keep, runs) in _selected(CASES3).items():
+    for name, case in _selected(CASES3).items():
+        (nx, ny, nz), seed, nt, keep, runs = case[:5]
         w, pos = tube_state(nx, ny, nz, seed)
         formats.write_ini(os.path.join(WORK, name + ".ini"), w, pos, gamma=GAMMA_REF,
                           g=(G3, 0.0, 0.0))
-        _build3(name, nx, ny, nz, nt)
+        _build3(name, nx, ny, nz, nt, case[5] if len(case) > 5 else None)
         print("prepared", name)
 
 
@@ -191,14 +200,17 @@ def run():
         _run_one(name, case[4])
         if name in TWICE:
             _run_one(name, case[4], "_r1")
-    for name, (n, seed, nt, keep, runs) in _selected(CASES3).items():
+    for name, case in _selected(CASES3).items():
+        keep, runs = case[3], case[4]
         for r in range(runs):
             _run_one(name, keep, "" if r == 0 else "_r%d" % r)
 
 
 def collect():
     from smaug_b200 import formats
-    for name, ((nx, ny, nz), seed, nt, keep, runs) in _selected(CASES3).items():
+    for name, case in _selected(CASES3).items():
+        (nx, ny, nz), seed, nt, keep, runs = case[:5]
+        extra = {"bt": np.array(case[6]), "bt_ref": np.array(case[5])} if len(case) > 6 else {}
         w0, pos0, _ = formats.read_ini(os.path.join(WORK, name + ".ini"), 3)
         states, times = [], []
         for k in keep:
@@ -209,7 +221,7 @@ def collect():
                             steps=np.array(keep), states=np.array(states),
                             hdr_t=np.array(times), gamma=GAMMA_REF,
                             dx=np.array([L3 / nx, L3 / ny, L3 / nz]),
-                            g=np.array([G3, 0.0, 0.0]))
+                            g=np.array([G3, 0.0, 0.0]), **extra)
         print("wrote", name)
     for name, case in _selected(CASES).items():
         nx, ny, seed, nt, keep = case[:5]

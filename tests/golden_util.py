@@ -10,7 +10,7 @@ STRICT = ("g16", "g18x12", "ot64")     # full multi-step runs
 BOUNDARY = ("f16x", "f18y")            # fixed ghosts along dim 0 / dim 1
 ONESTEP = ("ot24x20",)                 # consecutive steps, one-step parity
 RACE = ("ot128",)                      # 128^2, 200 steps, two runs of the reference
-STRICT3 = ("t3s", "t3a", "t3b")        # 3D flux-tube build, contcd4 ghosts, backgrounds
+STRICT3 = ("t3s", "t3a", "t3b", "t3f")  # 3D flux-tube build, contcd4 (t3f: fixed dim 0) ghosts
 
 
 def load(name):
@@ -29,9 +29,11 @@ def params(d, **kw):
     kw.setdefault("integrator", P.INT_EULER)
     if d["w0"].ndim == 4:
         nz, ny, nx = d["w0"].shape[1:]
+        bt = [int(b) for b in d["bt"]] if "bt" in d else [P.BC_CONTCD4] * 3
+        kw.setdefault("boundtype", bt)
         return P.make_params(ndim=3, n=(nx, ny, nz), dx=tuple(d["dx"]),
                              gamma=float(d["gamma"]), courant=0.3, dtmax=1.0, dt=1e-8,
-                             g=tuple(d["g"]), boundtype=[[P.BC_CONTCD4] * 2] * 3, **kw)
+                             g=tuple(d["g"]), **kw)
     ny, nx = d["w0"].shape[1:]
     if "bt" in d:
         kw.setdefault("boundtype", tuple(int(b) for b in d["bt"]))
