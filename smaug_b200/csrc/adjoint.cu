@@ -642,6 +642,21 @@ __global__ void __launch_bounds__(ANT, SMAUG_ADJ_MINB) adj_stage2d(const KParams
   const int n0 = P.n0, n1 = P.n1;
   const long nc = P.ncell;
   const double dt = I.dt;
+  const int gi = T.x0 + tx, gj = T.y0 + ty;
+  const bool active = gi <= n0 - 3 && gj <= n1 - 3;
+  const long co = (long)gj * n0 + gi;
+  double lam[6];
+  bool nonzero = false;
+#pragma unroll
+  for (int f = 0; f < 6; f++) {
+    lam[f] = active ? I.lam[f * nc + co] : 0.0;
+    nonzero |= lam[f] != 0.0;
+  }
+  // every term below is linear in the tile's k-bar: a tile without any adds
+  // nothing (sparse adjoints: a loss on part of the domain)
+  if (!__syncthreads_or(nonzero)) return;
+#pragma unroll
+  for (int f = 0; f < 6; f++) Lam[f * ANT + tid] = lam[f];
 
   // ---- stage X, backgrounds, 1/rho_t, zero the accumulator ---------------
   for (int r = tid; r < RC; r += ANT) {
@@ -670,15 +685,6 @@ __global__ void __launch_bounds__(ANT, SMAUG_ADJ_MINB) adj_stage2d(const KParams
       T.dl1[r - RX] = d;
       T.rd1[r - RX] = 1.0 / d;
     }
-  }
-  const int gi = T.x0 + tx, gj = T.y0 + ty;
-  const bool active = gi <= n0 - 3 && gj <= n1 - 3;
-  const long co = (long)gj * n0 + gi;
-  double lam[6];
-#pragma unroll
-  for (int f = 0; f < 6; f++) {
-    lam[f] = active ? I.lam[f * nc + co] : 0.0;
-    Lam[f * ANT + tid] = lam[f];
   }
   __syncthreads();
 
@@ -1145,6 +1151,7 @@ static int adj_create(const smaug_params_t* p, const double* w, const double* po
   A_TRY(cudaMalloc(&a->W, eb));
   A_TRY(cudaMalloc(&a->Kb, eb));
   A_TRY(cudaMalloc(&a->Xb, eb));
+  A_TRY(cudaMemset(a->Xb, 0, eb));
   A_TRY(cudaMalloc(&a->bg, sizeof(double) * 4 * nc));
   A_TRY(cudaMemcpy(a->bg, w + 6 * nc, sizeof(double) * 4 * nc, cudaMemcpyHostToDevice));
   for (int d = 0; d < 2; d++) {
@@ -1221,7 +1228,6 @@ static int adj_bwd(Adjoint* a, const double* u, const double* ubar_next, double*
     Xs = a->X;
   }
   const long nc = a->nc;
-  const size_t eb = sizeof(double) * 6 * nc;
   // CFL maxima of the four stage inputs and the cells that attain them
   CUDA_TRY(cudaMemsetAsync(a->mx, 0, sizeof(unsigned long long) * 8, st));
   CUDA_TRY(cudaMemsetAsync(a->arg, 0x7f, sizeof(int) * 8, st));
@@ -1235,6 +1241,7 @@ static int adj_bwd(Adjoint* a, const double* u, const double* ubar_next, double*
   CUDA_TRY(cudaMemsetAsync(thbar, 0, sizeof(double) * 3, st));
   const double dt = a->P.dt;
   const double ts[4] = {t, t + 0.5 * dt, t + 0.5 * dt, t + dt};
+  const size_t eb = sizeof(double) * 6 * nc;
   for (int s = 3; s >= 0; s--) {
     CUDA_TRY(cudaMemsetAsync(a->Xb, 0, eb, st));
     CUDA_TRY(cudaMemsetAsync(a->sbar, 0, sizeof(double) * 2, st));
