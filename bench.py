@@ -369,11 +369,12 @@ def _adjoint_case(args, sa, q, p, u0, pos, rhob, theta0, shift, obs_z, nsteps, r
     for _ in range(max(args.warmup, 1)):
         with torch.no_grad():
             rollout(sa, theta0, u0, 20, loss_fn, checkpoint_every=20)
-    # one short backward of each rollout outside the timed regions (the tape
-    # of 20 steps is allocated on the first backward)
+    # one full backward of each rollout outside the timed regions (the tape
+    # is allocated on the first backward, and torch's caching allocator
+    # grows to the rollout's working set)
     for fn in (rollout, rollout_autograd):
         thw = theta0.clone().requires_grad_(True)
-        fn(sa, thw, u0, 20, loss_fn, checkpoint_every=20).backward()
+        fn(sa, thw, u0, nsteps, loss_fn, checkpoint_every=20).backward()
     with torch.no_grad():
         L0, ms_fwd = timed(lambda: rollout(sa, theta0, u0, nsteps, loss_fn, checkpoint_every=20))
 
