@@ -45,7 +45,6 @@ import os
 import statistics
 import subprocess
 import sys
-import threading
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
@@ -105,32 +104,39 @@ class ClockSampler:
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, index=0):
+    def __init__(self, index=0, period_ms=50):
         self.index = index
+        self.period_ms = period_ms
         self.samples = []
-        self._stop = threading.Event()
-        self._t = threading.Thread(target=self._run, daemon=True)
-
-    def _run(self):
-        while not self._stop.is_set():
-            try:
-                out = subprocess.run(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
-                                      "--format=csv,noheader,nounits"],
-                                     capture_output=True, text=True, timeout=5).stdout
-                for ln in out.strip().splitlines():
-                    f = [x.strip() for x in ln.split(",")]
-                    self.samples.append(f)
-            except Exception:
-                pass
-            self._stop.wait(0.2)
+        self._p = None
 
     def __enter__(self):
-        self._t.start()
+        # one nvidia-smi in loop mode (-lms), the process this object started
+        try:
+            self._p = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                 "--format=csv,noheader,nounits", "-lms", str(self.period_ms)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            # the first sample arrives once nvidia-smi is up: the timed
+            # region starts after it, and it is not counted
+            self._p.stdout.readline()
+        except Exception:
+            self._p = None
         return self
 
     def __exit__(self, *a):
-        self._stop.set()
-        self._t.join(timeout=10)
+        if self._p is None:
+            return
+        self._p.terminate()
+        try:
+            out, _ = self._p.communicate(timeout=10)
+        except Exception:
+            self._p.kill()
+            out, _ = self._p.communicate()
+        for ln in (out or "").strip().splitlines():
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) >= 5:
+                self.samples.append(f)
 
     def summary(self):
         sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
