@@ -110,7 +110,7 @@ __global__ void cmax3d_kernel(const KParams P, const double* u, const double* bg
     double s[8], g[5];
     for (int f = 0; f < 8; f++) s[f] = u[f * nc + c];
     for (int f = 0; f < 5; f++) g[f] = bg[f * nc + c];
-    for (int d = 0; d < 3; d++) cm[d] = cfast3(P.gamma, s, g, d);
+    cfast3_all(P.gamma, s, g, cm);
   }
   for (int d = 0; d < 3; d++) {
     double v = cm[d];
@@ -128,10 +128,9 @@ __global__ void cmax2d_kernel(const KParams P, const double* u, const double* bg
   if (use && fixed_only) use = fixed_ghost(P, (int)(c % P.n0), (int)(c / P.n0), 0);
   if (use) {
     const long nc = P.ncell;
-    for (int d = 0; d < 2; d++)
-      cm[d] = cfast2(P.gamma, u[0 * nc + c], u[1 * nc + c], u[2 * nc + c], u[3 * nc + c],
-                     u[4 * nc + c], u[5 * nc + c], bg[0 * nc + c], bg[1 * nc + c], bg[2 * nc + c],
-                     bg[3 * nc + c], d);
+    cfast2_both(P.gamma, u[0 * nc + c], u[1 * nc + c], u[2 * nc + c], u[3 * nc + c], u[4 * nc + c],
+                u[5 * nc + c], bg[0 * nc + c], bg[1 * nc + c], bg[2 * nc + c], bg[3 * nc + c], cm[0],
+                cm[1]);
   }
   for (int d = 0; d < 2; d++) {
     double v = cm[d];

@@ -112,6 +112,14 @@ struct Form<true> {
 __device__ __forceinline__ double dmax0(double m, double v) { return (v > m) ? v : m; }
 template <typename T>
 __device__ __forceinline__ T hmax0(T m, T v) { return (v > m) ? v : m; }
+// quotient of the nu ratio (b > 0): IEEE division in double; in the float
+// arithmetic of the mixed form the fast reciprocal-based quotient (2 ulp, far
+// below the form's own rounding) for a normal divisor, IEEE division for a
+// subnormal one (whose fast reciprocal would overflow)
+__device__ __forceinline__ double hdiv(double a, double b) { return a / b; }
+__device__ __forceinline__ float hdiv(float a, float b) {
+  return b >= 1.17549435e-38f ? __fdividef(a, b) : a / b;
+}
 
 // dt rule, src/iosmaug.c:541-616 (a rejected candidate keeps the previous dt,
 // see the oracle's dt_rule for why)
@@ -128,22 +136,34 @@ __device__ __forceinline__ double device_dt(const KParams& P, const double* cmax
   return dt_prev;
 }
 
-// computec3 (src/dervfields.cu:241-309), 2D, fast speed along `dir`
+// computec3 (src/dervfields.cu:241-309), 2D: the fast speeds along both
+// dimensions from one state, sharing 1/rho_t, the pressure and the sound and
+// Alfven terms (the reference's divisions by rho_t are multiplications with
+// its reciprocal here; the results agree at rounding level)
+__device__ __forceinline__ void cfast2_both(double gamma, double rho, double m1, double m2, double e,
+                                            double b1, double b2, double eb, double rhob, double bb1,
+                                            double bb2, double& c0, double& c1) {
+  const double m2s = m1 * m1 + m2 * m2;
+  const double b2s = b1 * b1 + b2 * b2;
+  const double bbb = bb1 * b1 + bb2 * b2;
+  const double bb2s = bb1 * bb1 + bb2 * bb2;
+  const double r = 1.0 / (rho + rhob);
+  const double pk = (gamma - 1) * (e - 0.5 * (m2s * r) - 0.5 * b2s - bbb);
+  const double cs2 = (gamma * (pk + (gamma - 1) * (eb - 0.5 * bb2s))) * r;
+  const double cf = (b2s + bb2s + 2.0 * bbb) * r + cs2;
+  const double cf2 = cf * cf, k = 4.0 * cs2 * r;
+  const double bd0 = bb1 + b1, bd1 = bb2 + b2;
+  c0 = sqrt(0.5 * (cf + sqrt(cf2 - k * (bd0 * bd0)))) + fabs(m1 * r);
+  c1 = sqrt(0.5 * (cf + sqrt(cf2 - k * (bd1 * bd1)))) + fabs(m2 * r);
+}
+
+// the fast speed along `dir` alone
 __device__ __forceinline__ double cfast2(double gamma, double rho, double m1, double m2, double e,
                                          double b1, double b2, double eb, double rhob, double bb1,
                                          double bb2, int dir) {
-  double m2s = m1 * m1 + m2 * m2;
-  double b2s = b1 * b1 + b2 * b2;
-  double bbb = bb1 * b1 + bb2 * b2;
-  double bb2s = bb1 * bb1 + bb2 * bb2;
-  double rt = rho + rhob;
-  double pk = (gamma - 1) * (e - 0.5 * (m2s / rt) - 0.5 * b2s - bbb);
-  double cs2 = (gamma * (pk + (gamma - 1) * (eb - 0.5 * bb2s))) / rt;
-  double cf = (b2s + bb2s + 2.0 * bbb) / rt + cs2;
-  double bd = (dir == 0) ? (bb1 + b1) : (bb2 + b2);
-  double md = (dir == 0) ? m1 : m2;
-  double cfasti = 0.5 * (cf + sqrt(cf * cf - 4.0 * cs2 * (bd * bd) / rt));
-  return sqrt(cfasti) + fabs(md / rt);
+  double c0, c1;
+  cfast2_both(gamma, rho, m1, m2, e, b1, b2, eb, rhob, bb1, bb2, c0, c1);
+  return dir == 0 ? c0 : c1;
 }
 
 // ghost images of interior index a along a dimension of n cells (the
@@ -192,19 +212,31 @@ __device__ __forceinline__ bool zero1n(int a, int n) {
 enum { R3 = 0, M3 = 1, E3 = 4, B3 = 5 };            // m_c = M3 + c, b_c = B3 + c
 enum { GEB = 0, GRB = 1, GBB = 2 };                 // bb_c = GBB + c
 
-// computec3 (src/dervfields.cu:241-309), 3D, fast speed along `dir`
-__device__ __forceinline__ double cfast3(double gamma, const double* s, const double* g, int dir) {
+// computec3 (src/dervfields.cu:241-309), 3D: the fast speeds along the
+// three dimensions, sharing 1/rho_t and the sound and Alfven terms as
+// cfast2_both does
+__device__ __forceinline__ void cfast3_all(double gamma, const double* s, const double* g, double* c) {
   const double m2s = s[1] * s[1] + s[2] * s[2] + s[3] * s[3];
   const double b2s = s[5] * s[5] + s[6] * s[6] + s[7] * s[7];
   const double bbb = g[2] * s[5] + g[3] * s[6] + g[4] * s[7];
   const double bb2s = g[2] * g[2] + g[3] * g[3] + g[4] * g[4];
-  const double rt = s[0] + g[1];
-  const double pk = (gamma - 1) * (s[4] - 0.5 * (m2s / rt) - 0.5 * b2s - bbb);
-  const double cs2 = (gamma * (pk + (gamma - 1) * (g[0] - 0.5 * bb2s))) / rt;
-  const double cf = (b2s + bb2s + 2.0 * bbb) / rt + cs2;
-  const double bd = g[2 + dir] + s[5 + dir];
-  const double cfasti = 0.5 * (cf + sqrt(cf * cf - 4.0 * cs2 * (bd * bd) / rt));
-  return sqrt(cfasti) + fabs(s[1 + dir] / rt);
+  const double r = 1.0 / (s[0] + g[1]);
+  const double pk = (gamma - 1) * (s[4] - 0.5 * (m2s * r) - 0.5 * b2s - bbb);
+  const double cs2 = (gamma * (pk + (gamma - 1) * (g[0] - 0.5 * bb2s))) * r;
+  const double cf = (b2s + bb2s + 2.0 * bbb) * r + cs2;
+  const double cf2 = cf * cf, k = 4.0 * cs2 * r;
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    const double bd = g[2 + d] + s[5 + d];
+    c[d] = sqrt(0.5 * (cf + sqrt(cf2 - k * (bd * bd)))) + fabs(s[1 + d] * r);
+  }
+}
+
+// the fast speed along `dir` alone
+__device__ __forceinline__ double cfast3(double gamma, const double* s, const double* g, int dir) {
+  double c[3];
+  cfast3_all(gamma, s, g, c);
+  return c[dir];
 }
 
 // 4th-order centred derivative along the stride s (grad3dn, src/gradops.cu:437-602)

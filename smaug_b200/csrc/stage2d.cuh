@@ -61,6 +61,7 @@ struct T2 {
   double* rd1;   // [RY]
   void* U;       // union scratch
   int x0, y0;
+  bool inner;    // the staged region lies inside the grid and off its pads
   // field f of the reference numbering at region cell l, in double
   __device__ __forceinline__ double v(int f, int l) const {
     if (f < 6) return (double)S[f * RC + l];
@@ -146,6 +147,11 @@ __device__ __forceinline__ void stage_q2(const T2<BG, MIX>& T, const KParams& P,
   HT* Q = static_cast<HT*>(T.U);
   const int n0 = P.n0, n1 = P.n1;
   const long nc = P.ncell;
+  if (T.inner) {
+    for (int r = tid; r < RC; r += NTHREADS) Q[r] = (HT)hq_at<BG, MIX, KIND, COMP>(T, r);
+    __syncthreads();
+    return;
+  }
   for (int r = tid; r < RC; r += NTHREADS) {
     const int lx = r % RX, ly = r / RX;
     const int ci = T.x0 - HALO + lx, cj = T.y0 - HALO + ly;
@@ -226,7 +232,7 @@ __device__ __forceinline__ void hyper_pass(const T2<BG, MIX>& T, const KParams& 
       t4 = hmax0(t4, (HT)fabs((HT)3 * (q[k + 2] - q[k + 1]) - (q[k + 3] - q[k])));
 #pragma unroll
     for (int k = 0; k < 5; k++) t5 = hmax0(t5, (HT)fabs(q[k + 1] - q[k]));
-    RR[r] = (t5 > 0) ? t4 / t5 : (HT)0;
+    RR[r] = (t5 > 0) ? hdiv(t4, t5) : (HT)0;
   }
   __syncthreads();
   // (C) cross-term arrays (hyperdifmomsourcene2-4 / hyperdifbsourcene1b-4)
@@ -235,14 +241,14 @@ __device__ __forceinline__ void hyper_pass(const T2<BG, MIX>& T, const KParams& 
       const int lx = oxN + r % exN, ly = oyN + r / exN;
       const int ci = T.x0 - HALO + lx, cj = T.y0 - HALO + ly;
       HT c3 = 0, c4 = 0;
-      if (ci > 0 && ci < n0 - 1 && cj > 0 && cj < n1 - 1) {
+      if (T.inner || (ci > 0 && ci < n0 - 1 && cj > 0 && cj < n1 - 1)) {
         const int a = DIM == 0 ? ci : cj;
         const int l = ly * RX + lx;
         // grad13n along DIM of q
         HT g = ((Q[l + SQ] - Q[l - SQ]) * (HT)(DIM == 0 ? T.rd0[lx] : T.rd1[ly])) * (HT)0.5;
         if ((P.bt[DIM] != 0) && zero1n(a, nd)) g = 0;
         HT nsum = 0;
-        if (ci >= 2 && ci <= n0 - 3 && cj >= 2 && cj <= n1 - 3) {
+        if (T.inner || (ci >= 2 && ci <= n0 - 3 && cj >= 2 && cj <= n1 - 3)) {
           const int rr = ri(lx, ly);
           const HT c = (HT)(DIM == 0 ? T.dl0[lx] : T.dl1[ly]) * coef;
           nsum = c * RR[rr] + c * RR[rr - SR];
@@ -351,6 +357,9 @@ __device__ __forceinline__ void stage2d_body(const KParams& P, const KBufs& B, i
   T.x0 = 2 + bx * TX;
   T.y0 = 2 + by * TY;
   const int n0 = P.n0, n1 = P.n1;
+  // region columns x0-3 .. x0+TX+2 (rows likewise) inside [0, n-1]: no
+  // bounds or pad checks in the staging, flux and cross-term loops
+  T.inner = bx >= 1 && by >= 1 && T.x0 + TX + HALO <= n0 && T.y0 + TY + HALO <= n1;
   const long nc = P.ncell;
   const ST* uin = static_cast<const ST*>(B.uin);
 
@@ -358,7 +367,7 @@ __device__ __forceinline__ void stage2d_body(const KParams& P, const KBufs& B, i
   for (int r = tid; r < RC; r += NTHREADS) {
     const int lx = r % RX, ly = r / RX;
     const int gi = T.x0 - HALO + lx, gj = T.y0 - HALO + ly;
-    const bool in = gi >= 0 && gi < n0 && gj >= 0 && gj < n1;
+    const bool in = T.inner || (gi >= 0 && gi < n0 && gj >= 0 && gj < n1);
     const long c = (long)gj * n0 + gi;
     double rho = 0.0, rhob = 1.0;
 #pragma unroll
@@ -443,7 +452,7 @@ __device__ __forceinline__ void stage2d_body(const KParams& P, const KBufs& B, i
       const int lx = ox + r % ex, ly = oy + r / ex;
       const int ci = T.x0 - HALO + lx, cj = T.y0 - HALO + ly;
       double f5[5] = {0, 0, 0, 0, 0};
-      if (ci >= 0 && ci < n0 && cj >= 0 && cj < n1) {
+      if (T.inner || (ci >= 0 && ci < n0 && cj >= 0 && cj < n1)) {
         if (d == 0)
           flux_at<BG, MIX, 0>(T, P.gamma, ly * RX + lx, f5);
         else
@@ -582,8 +591,10 @@ __device__ __forceinline__ void stage2d_body(const KParams& P, const KBufs& B, i
         } else {
           eb = B.bg[0 * nc + cc]; rb = B.bg[1 * nc + cc]; b1b = B.bg[2 * nc + cc]; b2b = B.bg[3 * nc + cc];
         }
-        cm0 = dmax0(cm0, cfast2(P.gamma, r[RHO], r[M1], r[M2], r[EN], r[B1], r[B2], eb, rb, b1b, b2b, 0));
-        cm1 = dmax0(cm1, cfast2(P.gamma, r[RHO], r[M1], r[M2], r[EN], r[B1], r[B2], eb, rb, b1b, b2b, 1));
+        double c0, c1;
+        cfast2_both(P.gamma, r[RHO], r[M1], r[M2], r[EN], r[B1], r[B2], eb, rb, b1b, b2b, c0, c1);
+        cm0 = dmax0(cm0, c0);
+        cm1 = dmax0(cm1, c1);
       }
   }
   __shared__ double red[NTHREADS / 32][2];

@@ -83,6 +83,7 @@ struct Box3 {
   void* U;         // union scratch
   int* C;          // [BC] q source code per box cell (box_code)
   int o[3];        // global coordinate of box index 0 per axis
+  bool inner;      // the box lies inside the grid and off its pads
 };
 
 // q of a hyperdiffusion field from global memory (src/hyperdifvisc1r.cu:1225-1253)
@@ -226,7 +227,7 @@ __device__ __forceinline__ void hyper_pass3(const Box3& X, const KParams& P, con
       t4 = hmax0(t4, (HT)fabs((HT)3 * (q[k + 2] - q[k + 1]) - (q[k + 3] - q[k])));
 #pragma unroll
     for (int k = 0; k < 5; k++) t5 = hmax0(t5, (HT)fabs(q[k + 1] - q[k]));
-    RR[r] = (t5 > 0) ? t4 / t5 : (HT)0;
+    RR[r] = (t5 > 0) ? hdiv(t4, t5) : (HT)0;
   }
   __syncthreads();
   // (C) cross-term arrays (hyperdifmomsourcene2-4 / hyperdifbsourcene1b-4)
@@ -235,15 +236,16 @@ __device__ __forceinline__ void hyper_pass3(const Box3& X, const KParams& P, con
       const int lx = G0 + r % E0, ly = G1 + (r / E0) % E1, lz = G2 + r / (E0 * E1);
       const int g[3] = {X.o[0] + lx, X.o[1] + ly, X.o[2] + lz};
       HT c3 = 0, c4 = 0;
-      if (g[0] > 0 && g[0] < n[0] - 1 && g[1] > 0 && g[1] < n[1] - 1 && g[2] > 0 && g[2] < n[2] - 1) {
+      if (X.inner ||
+          (g[0] > 0 && g[0] < n[0] - 1 && g[1] > 0 && g[1] < n[1] - 1 && g[2] > 0 && g[2] < n[2] - 1)) {
         const int q0 = (lz * s3::BY + ly) * s3::BX + lx;
         const int la = DIM == 0 ? lx : (DIM == 1 ? ly : lz);
         // grad13n along DIM of q
         HT gq = ((Q[q0 + SD] - Q[q0 - SD]) * (HT)X.rd[DIM][la]) * (HT)0.5;
         if ((P.bt[DIM] != 0) && zero1n(g[DIM], n[DIM])) gq = 0;
         HT nsum = 0;
-        if (g[0] >= 2 && g[0] <= n[0] - 3 && g[1] >= 2 && g[1] <= n[1] - 3 && g[2] >= 2 &&
-            g[2] <= n[2] - 3) {
+        if (X.inner || (g[0] >= 2 && g[0] <= n[0] - 3 && g[1] >= 2 && g[1] <= n[1] - 3 && g[2] >= 2 &&
+                        g[2] <= n[2] - 3)) {
           const int rr = ridx(lx, ly, lz);
           const HT cc = (HT)X.dl[DIM][la] * coef;
           nsum = cc * RR[rr] + cc * RR[rr - RS];
@@ -379,7 +381,7 @@ __device__ __forceinline__ void flux_pass3(const Box3& X, const KParams& P, cons
     const int lx = G0 + r % E0, ly = G1 + (r / E0) % E1, lz = G2 + r / (E0 * E1);
     const int g0 = X.o[0] + lx, g1 = X.o[1] + ly, g2 = X.o[2] + lz;
     double f[7] = {0, 0, 0, 0, 0, 0, 0}, v[3] = {0, 0, 0};
-    if (g0 >= 0 && g0 < n[0] && g1 >= 0 && g1 < n[1] && g2 >= 0 && g2 < n[2]) {
+    if (X.inner || (g0 >= 0 && g0 < n[0] && g1 >= 0 && g1 < n[1] && g2 >= 0 && g2 < n[2])) {
       const long c = ((long)g2 * n[1] + g1) * n[0] + g0;
       double s[8], g[5] = {0, 0, 0, 0, 0};
 #pragma unroll
@@ -451,13 +453,17 @@ __global__ void __launch_bounds__(s3::NT, SMAUG_MINB3D) stage3d_fast(const KPara
   X.o[0] = 2 + blockIdx.x * s3::T0 - s3::H;
   X.o[1] = 2 + blockIdx.y * s3::T1 - s3::H;
   X.o[2] = 2 + blockIdx.z * s3::T2 - s3::H;
+  // box indices 0 .. B-1 of every axis inside [0, n-1]: no bounds or pad
+  // checks in the staging, flux and cross-term loops
+  X.inner = X.o[0] >= 0 && X.o[1] >= 0 && X.o[2] >= 0 && X.o[0] + s3::BX <= n[0] &&
+            X.o[1] + s3::BY <= n[1] && X.o[2] + s3::BZ <= n[2];
 
   // ---- 1/rho_t on the box and the per-axis metric ----------------------
   for (int r = tid; r < s3::BC; r += s3::NT) {
     const int lx = r % s3::BX, ly = (r / s3::BX) % s3::BY, lz = r / s3::BS2;
     const int g0 = X.o[0] + lx, g1 = X.o[1] + ly, g2 = X.o[2] + lz;
     double rinv = 1.0;
-    if (g0 >= 0 && g0 < n[0] && g1 >= 0 && g1 < n[1] && g2 >= 0 && g2 < n[2]) {
+    if (X.inner || (g0 >= 0 && g0 < n[0] && g1 >= 0 && g1 < n[1] && g2 >= 0 && g2 < n[2])) {
       const long c = ((long)g2 * n[1] + g1) * n[0] + g0;
       rinv = 1.0 / ((double)__ldg(u + c) + __ldg(B.bg + GRB * nc + c));
     }
@@ -628,8 +634,10 @@ __global__ void __launch_bounds__(s3::NT, SMAUG_MINB3D) stage3d_fast(const KPara
 #pragma unroll
             for (int f = 0; f < 5; f++) gg[f] = __ldg(B.bg + f * nc + cc);
           }
+          double cv[3];
+          cfast3_all(P.gamma, r, gg, cv);
 #pragma unroll
-          for (int d = 0; d < 3; d++) cm[d] = dmax0(cm[d], cfast3(P.gamma, r, gg, d));
+          for (int d = 0; d < 3; d++) cm[d] = dmax0(cm[d], cv[d]);
         }
   }
   __shared__ double red[s3::NT / 32][3];
