@@ -61,6 +61,29 @@ UNIT = "Mcell-updates/s"
 TRAFFIC_PER_CELL_STEP = {(2, "fp64"): 865.8, (2, "mixed"): 723.8, (3, "fp64"): 1482.3,
                          (3, "mixed"): 1230.8}
 
+# FP64 (and FP32) floating-point operations per interior cell per stage counted
+# by ncu (smsp__sass_thread_inst_executed_op_{dadd,dmul,dfma}_pred_on, an FMA
+# counting 2; profiles/fp64_flops_per_cell.md: 2D at 2048^2, 3D at 128^3)
+FLOP_PER_CELL_STAGE = {(2, "fp64"): (1208.0, 29.0), (2, "mixed"): (566.0, 424.0),
+                       (3, "fp64"): (3731.0, 107.0)}
+
+
+def fp64_roofline(ndim, prec, ncell, steps, ms):
+    """Secondary roofline of a stage kernel against the nominal FP64 vector
+    peak (148 SMs x 64 FP64 FMA per clock x 2 at the maximum SM clock)."""
+    fl = FLOP_PER_CELL_STAGE.get((ndim, prec))
+    if fl is None:
+        return None
+    mhz = 1965.0
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        mhz = float(json.load(open(path)).get("sm_max_mhz", mhz))
+    peak = 148 * 64 * 2 * mhz * 1e6 / 1e12
+    ach = fl[0] * 4 * ncell * steps / (ms / 1e3) / 1e12
+    return {"bound": "fp64", "achieved": ach, "peak": peak, "unit": "TFLOP/s", "frac": ach / peak,
+            "fp64_flop_per_cell_stage": fl[0], "fp32_flop_per_cell_stage": fl[1],
+            "peak_kind": "nominal: 148 SMs x 64 FP64 FMA/clk x 2 x %.0f MHz" % mhz}
+
 
 def alg_bytes_per_cell_step(ndim):
     """Algorithmic HBM bytes per interior cell per RK4 step, FP64, by the
@@ -681,7 +704,8 @@ def main():
                  "roofline": {"bound": "hbm", "achieved": mach, "peak": peak_m, "unit": "GB/s",
                               "frac": mach / peak_m, "alg_bytes_per_cell_step": mbytes,
                               "scheme_bytes_per_cell_step": scheme_bytes_per_cell_step(p.ndim, True),
-                              "traffic": TRAFFIC_PER_CELL_STEP[(p.ndim, "mixed")] * ncell_int / 4}}
+                              "traffic": TRAFFIC_PER_CELL_STEP[(p.ndim, "mixed")] * ncell_int / 4},
+                 "fp64_roofline": fp64_roofline(p.ndim, "mixed", ncell_int, args.steps, mms)}
 
     if rank == 0:
         peak, pk_kind = peaks()
@@ -710,6 +734,7 @@ def main():
                          "alg_bytes_per_cell_step": alg_bytes,
                          "scheme_bytes_per_cell_step": scheme_bytes_per_cell_step(p.ndim),
                          "note": "stage kernel; FP64 arithmetic, not HBM, limits this form"},
+            "fp64_roofline": fp64_roofline(p.ndim, args.precision, ncell_int, args.steps, ms_max),
             "clocks": clk.summary(),
             "mixed": mixed,
         }
