@@ -360,7 +360,8 @@ def adjoint_main(args):
             line = res
         else:
             line["observation_row_0p4Mm"] = {k: res[k] for k in (
-                "value", "loss", "grad", "fd", "fd_rel_err", "forward_ms", "forward_backward_ms")}
+                "value", "loss", "grad", "fd", "fd_rel_err", "forward_ms", "forward_backward_ms",
+                "full_tape")}
             line["observation_row_0p4Mm"]["config_observed_row_z_m"] = res["config"]["observed_row_z_m"]
     sa.close()
     print(json.dumps(line), flush=True)
@@ -401,9 +402,9 @@ def _adjoint_case(args, sa, q, p, u0, pos, rhob, theta0, shift, obs_z, nsteps, r
     # one full backward of each rollout outside the timed regions (the tape
     # is allocated on the first backward, and torch's caching allocator
     # grows to the rollout's working set)
-    for fn in (rollout, rollout_autograd):
+    for fn, every in ((rollout, 20), (rollout_autograd, 20), (rollout, 0)):
         thw = theta0.clone().requires_grad_(True)
-        fn(sa, thw, u0, nsteps, loss_fn, checkpoint_every=20).backward()
+        fn(sa, thw, u0, nsteps, loss_fn, checkpoint_every=every).backward()
     with torch.no_grad():
         L0, ms_fwd = timed(lambda: rollout(sa, theta0, u0, nsteps, loss_fn, checkpoint_every=20))
 
@@ -422,6 +423,14 @@ def _adjoint_case(args, sa, q, p, u0, pos, rhob, theta0, shift, obs_z, nsteps, r
         return th.grad.clone()
 
     grad_c, ms_fb_c = timed(fwd_bwd_composed)
+
+    def fwd_bwd_full_tape():
+        th = theta0.clone().requires_grad_(True)
+        L = rollout(sa, th, u0, nsteps, loss_fn, checkpoint_every=0)
+        L.backward()
+        return th.grad.clone()
+
+    grad_t, ms_fb_t = timed(fwd_bwd_full_tape)
     fd = []
     for k in range(3):
         h = 1e-4 * float(theta0[k])
@@ -450,6 +459,14 @@ def _adjoint_case(args, sa, q, p, u0, pos, rhob, theta0, shift, obs_z, nsteps, r
             "grad": [float(g) for g in grad_c],
             "note": "single-step Functions under torch.utils.checkpoint; each step adjoint "
                     "recomputes its stage inputs"},
+        "full_tape": {
+            "value": ms_fb_t / ms_fwd, "forward_backward_ms": ms_fb_t,
+            "grad": [float(g) for g in grad_t],
+            "grad_max_rel_diff_vs_checkpointed": float((grad_t - grad).abs().max() / grad.abs().max())
+            if float(grad.abs().max()) > 0 else float((grad_t - grad).abs().max()),
+            "tape_bytes": 4 * 6 * p.ncells * 8 * nsteps,
+            "note": "checkpoint_every=0: the forward pass records every step's stage inputs "
+                    "(device tape), the backward recomputes nothing"},
     }
     return line
 

@@ -116,51 +116,80 @@ class Step(torch.autograd.Function):
 
 class _Rollout(torch.autograd.Function):
     """L = sum_n loss_fn(u_n, n) over a rollout, with the hand-written step
-    adjoint applied segment by segment from a tape."""
+    adjoint applied segment by segment from a tape (every > 0: checkpoints
+    every `every` steps, each segment recomputed into the tape in the
+    backward pass; every == 0: the forward pass records the tape of the whole
+    rollout and the backward pass recomputes nothing)."""
 
     @staticmethod
     def forward(ctx, theta, u0, sa, nsteps, loss_fn, t0, every):
         dt = sa.dt
         sa.set_driver(*theta.detach().cpu().tolist())
-        ckpt = []
+        ckpt, states = [], None
         total = torch.zeros((), dtype=torch.float64, device=u0.device)
         u = u0.detach()
         with torch.no_grad():
-            for n in range(nsteps):
-                if n % every == 0:
-                    ckpt.append(u)
-                u = sa.forward(u, t0 + n * dt)
-                total = total + loss_fn(u, n + 1)
+            if every == 0:
+                sa.reserve(nsteps)
+                states = [u]
+                for n in range(nsteps):
+                    u = sa.forward_tape(u, t0 + n * dt, n)
+                    states.append(u)
+                    total = total + loss_fn(u, n + 1)
+            else:
+                for n in range(nsteps):
+                    if n % every == 0:
+                        ckpt.append(u)
+                    u = sa.forward(u, t0 + n * dt)
+                    total = total + loss_fn(u, n + 1)
         ctx.sa, ctx.nsteps, ctx.loss_fn, ctx.t0, ctx.every = sa, nsteps, loss_fn, t0, every
-        ctx.ckpt = ckpt
+        ctx.ckpt, ctx.states = ckpt, states
         ctx.theta = theta.detach().cpu().tolist()
         ctx.theta_meta = (theta.dtype, theta.device)
         return total
+
+    @staticmethod
+    def _loss_grads(loss_fn, states, s):
+        """d loss_fn(u_n, n) / d u_n for the states u_{s+1}.. of a segment, in
+        one autograd call (each term depends on its own state only)."""
+        with torch.enable_grad():
+            us = [x.detach().requires_grad_(True) for x in states[1:]]
+            tot = None
+            for k, uk in enumerate(us):
+                lk = loss_fn(uk, s + k + 1)
+                tot = lk if tot is None else tot + lk
+            if tot is None or not tot.requires_grad:
+                return [None] * len(us)
+            return list(torch.autograd.grad(tot, us, allow_unused=True))
 
     @staticmethod
     def backward(ctx, gL):
         sa, nsteps, every, t0 = ctx.sa, ctx.nsteps, ctx.every, ctx.t0
         dt = sa.dt
         sa.set_driver(*ctx.theta)
-        sa.reserve(min(every, nsteps))
         ubar = None
         thbar = torch.zeros(3, dtype=torch.float64, device=gL.device)
-        for si in range(len(ctx.ckpt) - 1, -1, -1):
-            s = si * every
-            e = min(nsteps, s + every)
-            states = [ctx.ckpt[si]]
-            with torch.no_grad():
-                for n in range(s, e):
-                    states.append(sa.forward_tape(states[-1], t0 + n * dt, n - s))
+        if every == 0:
+            segments = [(0, nsteps, ctx.states, 0)]
+        else:
+            sa.reserve(min(every, nsteps))
+            segments = [(si * every, min(nsteps, si * every + every), None, si * every)
+                        for si in range(len(ctx.ckpt))]
+        for s, e, states, base in reversed(segments):
+            if states is None:
+                # recompute the segment into the tape (slots 0 .. e-s-1)
+                states = [ctx.ckpt[s // every]]
+                with torch.no_grad():
+                    for n in range(s, e):
+                        states.append(sa.forward_tape(states[-1], t0 + n * dt, n - s))
+            grads = _Rollout._loss_grads(ctx.loss_fn, states, s)
             for n in range(e - 1, s - 1, -1):
-                # d loss_fn(u_{n+1}, n+1) / d u_{n+1}
-                with torch.enable_grad():
-                    un = states[n - s + 1].detach().requires_grad_(True)
-                    gl, = torch.autograd.grad(ctx.loss_fn(un, n + 1), un, allow_unused=True)
-                g = gl * gL if gl is not None else torch.zeros_like(un)
+                gl = grads[n - s]
+                g = gl * gL if gl is not None else torch.zeros_like(states[n - s + 1])
                 ubar = g if ubar is None else ubar + g
-                ubar, tb = sa.backward_tape(n - s, ubar, t0 + n * dt)
+                ubar, tb = sa.backward_tape(n - base, ubar, t0 + n * dt)
                 thbar = thbar + tb
+        ctx.states = None
         dtype, device = ctx.theta_meta
         # ubar and thbar already carry the factor gL (it scales every loss gradient)
         return thbar.to(device=device, dtype=dtype), ubar, None, None, None, None, None
@@ -168,11 +197,16 @@ class _Rollout(torch.autograd.Function):
 
 def rollout(sa, theta, u0, nsteps, loss_fn, t0=0.0, checkpoint_every=20):
     """sum over steps n = 1..nsteps of loss_fn(u_n, n), differentiable in
-    theta and u0.  Keeps every `checkpoint_every`-th state; the backward
-    recomputes each segment once into a tape of its stage inputs
+    theta and u0.  With checkpoint_every = k > 0 it keeps every k-th state;
+    the backward recomputes each segment once into a tape of its stage inputs
     (smaug_adj_forward_tape) and applies the step adjoints from it
-    (smaug_adj_backward_tape), so no step is computed more than twice."""
-    return _Rollout.apply(theta, u0, sa, nsteps, loss_fn, t0, max(1, int(checkpoint_every)))
+    (smaug_adj_backward_tape), so no step is computed more than twice.  With
+    checkpoint_every = 0 the forward pass records the tape of all nsteps steps
+    (4 x nvar_evolved x cells doubles per step on the device) and the
+    backward recomputes nothing.  The loss gradients of a segment are taken
+    in one autograd call."""
+    every = 0 if not checkpoint_every else max(1, int(checkpoint_every))
+    return _Rollout.apply(theta, u0, sa, nsteps, loss_fn, t0, every)
 
 
 def rollout_autograd(sa, theta, u0, nsteps, loss_fn, t0=0.0, checkpoint_every=20):

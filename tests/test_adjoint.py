@@ -174,3 +174,34 @@ def test_taped_rollout_equals_checkpointed_composition(engine_lib):
     assert float((u1 - u2).norm()) <= 1e-10 * float(u2.norm())
     assert float(u2.norm()) > 0
     sa.close()
+
+
+def test_full_tape_rollout_equals_checkpointed(engine_lib):
+    """checkpoint_every = 0 (the forward pass records the tape of every step,
+    the backward recomputes nothing) gives the loss of the checkpointed
+    rollout exactly and its gradients to rounding (the same stage inputs and
+    step adjoints; the adjoint's reductions add in hardware order)."""
+    import torch
+    from smaug_b200.adjoint import rollout
+    sa, q, w, pos, u0 = setup(engine_lib, slab, 1)
+    kz = int(np.argmin(np.abs(pos[0][0] - 0.4e6)))
+    rhob = torch.tensor(w[7], device="cuda", dtype=torch.float64)
+    theta0 = torch.tensor([200.0, 30.0, 1.0e6], dtype=torch.float64)
+
+    def loss_fn(u, n):
+        v = u[1, :, kz] / (u[0, :, kz] + rhob[:, kz])
+        return (v ** 2).sum() * (1.0 + 0.1 * n)
+
+    out = []
+    for every in (4, 0):
+        th = theta0.clone().requires_grad_(True)
+        u = u0.clone().requires_grad_(True)
+        L = rollout(sa, th, u, 9, loss_fn, checkpoint_every=every)
+        L.backward()
+        out.append((float(L), th.grad.clone(), u.grad.clone()))
+    (L1, g1, u1), (L2, g2, u2) = out
+    assert L1 == L2
+    assert float((g1 - g2).abs().max()) <= 1e-12 * float(g2.abs().max())
+    assert float((u1 - u2).norm()) <= 1e-12 * float(u2.norm())
+    assert float(u2.norm()) > 0
+    sa.close()
