@@ -201,10 +201,12 @@ def workload(args, seed=1):
     prec = 1 if args.precision == "mixed" else 0
     if args.workload == "tube":
         p, w, pos = make_tube(N, seed, prec)
+        p.stencil_order = args.stencil_order
         return p, w, pos, N ** 3, ("3D stratified atmosphere %dx%dx%d (+2 ghost layers), 2x2x6 Mm, "
                                    "contcd4 vertical / periodic horizontal, gravity, Gaussian "
                                    "driver, hyperdiffusion, CFL 0.3, FP64, classical RK4" % (N, N, N))
     p, w, pos = make_case(N, seed, prec)
+    p.stencil_order = args.stencil_order
     return p, w, pos, N * N, ("2D Orszag-Tang %dx%d (+2 ghost layers), periodic, "
                               "hyperdiffusion, CFL 0.3, FP64, classical RK4" % (N, N))
 
@@ -588,6 +590,8 @@ def main():
     ap.add_argument("--precision", default=None, choices=["fp64", "mixed"],
                     help="default: fp64 (ot, tube; mixed reported beside it), mixed (ensemble)")
     ap.add_argument("--n", type=int, default=None)
+    ap.add_argument("--stencil-order", type=int, default=4, choices=[4, 6],
+                    help="flux derivative order (6: the reference's USE_DORDER3 build)")
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--ref-sample", type=int, default=512)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -735,6 +739,7 @@ def main():
             "dtype": "f64", "data": "synthetic",
             "config": {"workload": desc,
                        "interior_cells": ncell_int, "integrator": "rk4", "precision": "fp64",
+                       "stencil_order": args.stencil_order,
                        "parallelism": "replicas" if ws > 1 else "single-gpu",
                        "l2": "state %.2f GB per buffer > 126 MB L2, no flush" % state_gb},
             "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d,

@@ -97,7 +97,10 @@ typedef struct smaug_params {
   int32_t pad_model;        /* SMAUG_PAD_* */
   int32_t boundtype[3][2];  /* p->boundtype[*][dim][0]=upper, [1]=lower */
   int32_t driver;           /* SMAUG_DRIVER_* */
-  int32_t reserved_i[7];
+  int32_t stencil_order;    /* flux-divergence derivative grad3dn: 4 (or 0) the
+                               4th-order default, 6 the reference's USE_DORDER3
+                               build (src/gradops.cu:450-453) */
+  int32_t reserved_i[6];
   double dx[3];             /* p->dx: (xmax-xmin)/(n-4), used by the dt rule */
   double dt;                /* p->dt at start (the reference sets 1e-8 when moddton) */
   double dtmax;             /* DT: adaptive dt is accepted only below this */

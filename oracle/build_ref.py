@@ -117,14 +117,14 @@ def _configure(tmp, ni, nj, nt, nk, cfg):
     return src, inc
 
 
-def _driver_objects(src, three, verbose):
+def _driver_objects(src, three, verbose, defines=()):
     """The reference's host driver (g++, as src/make_inputs:3 selects)."""
     sac = "-DUSE_SAC_3D" if three else "-DUSE_SAC"
     objs = []
     for c in (CFILES_3D if three else CFILES):
         o = os.path.join(src, c.rsplit(".", 1)[0] + ".o")
-        cmd = ["g++", "-O0", "-fno-unreachable-traps", sac, "-DD1D", "-w", "-fpermissive",
-               "-o", o, "-c", os.path.join(src, c)]
+        cmd = ["g++", "-O0", "-fno-unreachable-traps", sac, "-DD1D", "-w", "-fpermissive"] + \
+            ["-D" + d for d in defines] + ["-o", o, "-c", os.path.join(src, c)]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.check_call(cmd, cwd=src)
@@ -141,7 +141,10 @@ def _cached(name, stamp):
     return binp, stampf, fresh
 
 
-def build_ref(name, ni, nj, nt, arch="sm_100a", verbose=True, nk=None, **kw):
+def build_ref(name, ni, nj, nt, arch="sm_100a", verbose=True, nk=None, defines=(), **kw):
+    """Build the reference's GPU binary for an ni x nj (x nk) grid and nt
+    steps; `defines` are extra build macros of the reference (e.g.
+    USE_DORDER3, the 6th-order flux derivative), kw override iosmaugparams.h."""
     if not os.path.isdir(REFROOT):
         raise RuntimeError("reference sources not present at %s" % REFROOT)
     cfg = dict(DEFAULTS)
@@ -149,7 +152,8 @@ def build_ref(name, ni, nj, nt, arch="sm_100a", verbose=True, nk=None, **kw):
     three = nk is not None
     if three and nk > nj:
         raise ValueError("3D reference builds need nk <= nj")
-    stamp = "ni=%d nj=%d nk=%s nt=%d %s arch=%s\n" % (ni, nj, nk, nt, sorted(cfg.items()), arch)
+    stamp = "ni=%d nj=%d nk=%s nt=%d %s arch=%s%s\n" % (ni, nj, nk, nt, sorted(cfg.items()), arch,
+                                                     "".join(" -D" + d for d in defines))
     binp, stampf, fresh = _cached(name, stamp)
     if fresh:
         return binp
@@ -174,13 +178,13 @@ def build_ref(name, ni, nj, nt, arch="sm_100a", verbose=True, nk=None, **kw):
         for cu in MODIDS:
             o = os.path.join(src, cu[:-3] + ".o")
             cmd = ["nvcc", "-arch=" + arch, "-maxrregcount=32", sac, "-w",
-                   "-Xcompiler", "-fno-unreachable-traps",
-                   "-o", o, "-c", os.path.join(src, cu)]
+                   "-Xcompiler", "-fno-unreachable-traps"] + ["-D" + d for d in defines] + \
+                  ["-o", o, "-c", os.path.join(src, cu)]
             if verbose:
                 print(" ".join(cmd), flush=True)
             subprocess.check_call(cmd, cwd=src)
             objs.append(o)
-        objs += _driver_objects(src, three, verbose)
+        objs += _driver_objects(src, three, verbose, defines)
         cmd = ["nvcc", "-arch=" + arch, "-o", binp] + objs + ["-lcudart", "-lm"]
         if verbose:
             print(" ".join(cmd), flush=True)

@@ -181,15 +181,26 @@ static inline long stepd(const O *o, int dir) {
   return dir == 0 ? 1 : (dir == 1 ? o->n[0] : (long)o->n[0] * o->n[1]);
 }
 
-/* grad3dn_MODID: 4th-order centred derivative, src/gradops.cu:437-602 */
+/* grad3dn_MODID: 4th-order centred derivative, src/gradops.cu:437-602; the
+   6th-order form of the USE_DORDER3 build (stencil_order 6,
+   src/gradops.cu:450-453) is defined on x in (2, n-3) only.  In 2D the
+   reference's dir-1 branch has no #else after its USE_DORDER3 block
+   (src/gradops.cu:536-544): the 4th-order form that follows overwrites it,
+   so a 2D build is 6th order along dim 0 and 4th order along dim 1. */
 static double grad3dn(const O *o, const double *a, const int *ii, int field, int dir) {
   double grad = 0;
   int x = ii[dir], n = o->n[dir];
   long c = E(o, ii[0], ii[1], ii[2]);
   long s = stepd(o, dir);
-  if (x > 1 && x < n - 2)
+  if (o->P->stencil_order == 6 && !(o->nd == 2 && dir == 1)) {
+    if (x > 2 && x < n - 3)
+      grad = (((3 * a[c + s] - 3 * a[c - s] + 3.0 * (a[c - 2 * s] - a[c + 2 * s]) / 5.0 -
+                (a[c - 3 * s] - a[c + 3 * s]) / 15.0) / 2.0)) /
+             (2.0 * (o->wd[F(o, o->delx[dir]) + c]));
+  } else if (x > 1 && x < n - 2) {
     grad = ((8 * a[c + s] - 8 * a[c - s] + a[c - 2 * s] - a[c + 2 * s]) / 6.0) /
            (2.0 * (o->wd[F(o, o->delx[dir]) + c]));
+  }
   (void)field;
   if (bt0(o, dir) != 0) {
     /* C precedence: a || (b && c && ...) (src/gradops.cu:463-474) */

@@ -87,6 +87,9 @@ void create_engine(const params* p, double dtmax) {
   const char* prec = std::getenv("SMAUG_COMPAT_PRECISION");
   if (prec && !std::strcmp(prec, "mixed")) ep.precision = SMAUG_PREC_MIXED;
   ep.pad_model = SMAUG_PAD_STRAY;
+#ifdef USE_DORDER3
+  ep.stencil_order = 6;  // the reference's 6th-order grad3dn build (src/gradops.cu:450-453)
+#endif
   for (int d = 0; d < ND; d++)
     for (int s = 0; s < 2; s++) {
       for (int f = 1; f < NV; f++)

@@ -229,6 +229,8 @@ static int validate(const smaug_params_t* p) {
   if (!(p->gamma > 1.0)) return set_error(SMAUG_E_INVALID, "gamma must be > 1");
   if (p->driver != SMAUG_DRIVER_NONE && p->driver != SMAUG_DRIVER_GAUSS)
     return set_error(SMAUG_E_INVALID, "unknown driver %d", p->driver);
+  if (p->stencil_order != 0 && p->stencil_order != 4 && p->stencil_order != 6)
+    return set_error(SMAUG_E_INVALID, "stencil_order must be 4 or 6 (got %d)", p->stencil_order);
   return SMAUG_OK;
 }
 
@@ -328,6 +330,7 @@ static int create(const smaug_params_t* p, const double* w, const double* pos, E
   K.n2 = n2;
   K.ncell = nc;
   set_boundaries(K, p, e->nd);
+  K.order6 = p->stencil_order == 6;
   for (int d = 0; d < 3; d++) {
     K.dx[d] = p->dx[d];
     K.g[d] = p->g[d];
@@ -884,6 +887,8 @@ static int batch_create(int nruns, const smaug_params_t* const* params, const do
       return fail(set_error(SMAUG_E_UNSUPPORTED, "run %d: batches step with RK4", r));
     if (params[r]->precision != params[0]->precision)
       return fail(set_error(SMAUG_E_UNSUPPORTED, "run %d: all runs of a batch share one precision form", r));
+    if (params[r]->stencil_order == 6)
+      return fail(set_error(SMAUG_E_UNSUPPORTED, "run %d: batches use the 4th-order stencil", r));
     Engine* e = nullptr;
     int rc = create(params[r], w[r], pos[r], &e);
     if (rc) return fail(rc);
@@ -1197,6 +1202,7 @@ extern "C" int smaug_euler_step_noalloc(const smaug_params_t* p, const double* w
   K.n2 = 1;
   K.ncell = nc;
   set_boundaries(K, p, 2);
+  K.order6 = p->stencil_order == 6;
   for (int d = 0; d < 3; d++) {
     K.dx[d] = p->dx[d];
     K.g[d] = p->g[d];

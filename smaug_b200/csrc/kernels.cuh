@@ -48,6 +48,7 @@ struct KParams {
   double g[3];
   double chyp[SMAUG_MAXVAR];
   int moddton, hyperdif, has_bg, has_grav, driver;
+  int order6;       // 1: 6th-order flux derivative (the reference's USE_DORDER3)
   double drv_amp, drv_period, drv_x0[3], drv_sigma[3];
 };
 
@@ -243,6 +244,21 @@ __device__ __forceinline__ double cfast3(double gamma, const double* s, const do
 __device__ __forceinline__ double d4(const double* a, int l, int s, double rdl2) {
   return ((8.0 * (a[l + s] - a[l - s]) + (a[l - 2 * s] - a[l + 2 * s])) * (1.0 / 6.0)) * rdl2;
 }
+
+// 6th-order centred derivative of the USE_DORDER3 build (grad3dn,
+// src/gradops.cu:450-453): (3 (a+1 - a-1) + 3/5 (a-2 - a+2) - (a-3 - a+3)/15) / 2 / (2 dx)
+__device__ __forceinline__ double d6(const double* a, int l, int s, double rdl2) {
+  return ((3.0 * (a[l + s] - a[l - s]) + 0.6 * (a[l - 2 * s] - a[l + 2 * s]) -
+           (a[l - 3 * s] - a[l + 3 * s]) * (1.0 / 15.0)) * 0.5) * rdl2;
+}
+// the flux derivative of the selected order
+template <bool O6>
+__device__ __forceinline__ double dflux(const double* a, int l, int s, double rdl2) {
+  return O6 ? d6(a, l, s, rdl2) : d4(a, l, s, rdl2);
+}
+// cells of the interior where the 6th-order derivative is undefined and
+// grad3dn leaves 0: the first and last interior index (x in (2, n-3) only)
+__device__ __forceinline__ bool edge6(int a, int n) { return a == 2 || a == n - 3; }
 
 // base state of a field value (the RK4 base / the Euler input) in double
 template <bool MIX>

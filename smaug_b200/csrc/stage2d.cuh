@@ -31,20 +31,27 @@
 
 // (included inside namespace smaug)
 namespace s2 {
-constexpr int FSZ = (TX + 4) * TY > TX * (TY + 4) ? (TX + 4) * TY : TX * (TY + 4);
+// flux arrays: the tile +-2 along the direction (+-3 along dim 0 for the
+// 6th-order derivative, which a 2D build of the reference applies along dim 0
+// only: its dir-1 USE_DORDER3 branch is overwritten by the 4th-order form,
+// src/gradops.cu:536-544)
+template <bool O6>
+__host__ __device__ constexpr int fsz() {
+  return (TX + (O6 ? 6 : 4)) * TY > TX * (TY + 4) ? (TX + (O6 ? 6 : 4)) * TY : TX * (TY + 4);
+}
 constexpr int RSZ = (TX + 1) * (TY + 2) > (TX + 2) * (TY + 1) ? (TX + 1) * (TY + 2) : (TX + 2) * (TY + 1);
 constexpr int NSZ = TX * (TY + 2) > (TX + 2) * TY ? TX * (TY + 2) : (TX + 2) * TY;
 constexpr int HYP = RC + RSZ + 2 * NSZ;  // q, ratio, two cross-term arrays
-template <bool MIX>
+template <bool MIX, bool O6 = false>
 __host__ __device__ constexpr size_t union_bytes() {
-  return (5 * FSZ * sizeof(double)) > HYP * sizeof(typename Form<MIX>::H)
-             ? 5 * FSZ * sizeof(double)
+  return (5 * fsz<O6>() * sizeof(double)) > HYP * sizeof(typename Form<MIX>::H)
+             ? 5 * fsz<O6>() * sizeof(double)
              : HYP * sizeof(typename Form<MIX>::H);
 }
-template <bool BG, bool MIX>
+template <bool BG, bool MIX, bool O6 = false>
 __host__ __device__ constexpr size_t smem_bytes() {
   return 6 * RC * sizeof(typename Form<MIX>::S) +
-         sizeof(double) * ((BG ? 6 : 0) * RC + RC + 2 * (RX + RY)) + union_bytes<MIX>();
+         sizeof(double) * ((BG ? 6 : 0) * RC + RC + 2 * (RX + RY)) + union_bytes<MIX, O6>();
 }
 }  // namespace s2
 
@@ -336,7 +343,7 @@ __device__ __forceinline__ void hyper_pass(const T2<BG, MIX>& T, const KParams& 
 
 // The stage for tile (bx, by) of one grid; the single-run kernel below and
 // the batched kernel (batch.cu) call it.
-template <int MODE, bool BG, bool MIX>
+template <int MODE, bool BG, bool MIX, bool O6 = false>
 __device__ __forceinline__ void stage2d_body(const KParams& P, const KBufs& B, int bx, int by) {
   using ST = typename Form<MIX>::S;
   extern __shared__ double smem[];
@@ -443,10 +450,13 @@ __device__ __forceinline__ void stage2d_body(const KParams& P, const KBufs& B, i
   }
 
   // ---- fluxes and divergence (centdiff1 / centdiff2), direction 0 then 1 --
+  constexpr int FSZ = s2::fsz<O6>();
 #pragma unroll
   for (int d = 0; d < 2; d++) {
-    const int ex = (d == 0) ? TX + 4 : TX, ey = (d == 0) ? TY : TY + 4;
-    const int ox = (d == 0) ? 1 : HALO, oy = (d == 0) ? HALO : 1;
+    const bool o6d = O6 && d == 0;  // 6th order along dim 0 only (see s2::fsz)
+    const int fh = o6d ? 3 : 2;     // flux halo along the direction
+    const int ex = (d == 0) ? TX + 2 * fh : TX, ey = (d == 0) ? TY : TY + 2 * fh;
+    const int ox = (d == 0) ? HALO - fh : HALO, oy = (d == 0) ? HALO : HALO - fh;
     double* F = static_cast<double*>(T.U);
     for (int r = tid; r < ex * ey; r += NTHREADS) {
       const int lx = ox + r % ex, ly = oy + r / ex;
@@ -459,19 +469,19 @@ __device__ __forceinline__ void stage2d_body(const KParams& P, const KBufs& B, i
           flux_at<BG, MIX, 1>(T, P.gamma, ly * RX + lx, f5);
       }
 #pragma unroll
-      for (int k = 0; k < 5; k++) F[k * s2::FSZ + r] = f5[k];
+      for (int k = 0; k < 5; k++) F[k * FSZ + r] = f5[k];
     }
     __syncthreads();
     if (active) {
       const int a = d == 0 ? gi : gj, n = d == 0 ? n0 : n1;
-      const bool z = (P.bt[d] != 0) && zero3dn(a, n);
+      const bool z = ((P.bt[d] != 0) && zero3dn(a, n)) || (o6d && edge6(a, n));
       const double rdl2 = 0.5 * (d == 0 ? T.rd0[lxo] : T.rd1[lyo]);
       const int fo = (lyo - oy) * ex + (lxo - ox);
       const int fs = d == 0 ? 1 : ex;
       const int fld[5] = {RHO, M1, M2, EN, d == 0 ? B2 : B1};
 #pragma unroll
       for (int k = 0; k < 5; k++) {
-        double g = d4(F + k * s2::FSZ, fo, fs, rdl2);
+        double g = o6d ? d6(F + k * FSZ, fo, fs, rdl2) : d4(F + k * FSZ, fo, fs, rdl2);
         if (z) g = 0;
         out[fld[k]] = out[fld[k]] - dt * g;
       }
@@ -480,12 +490,12 @@ __device__ __forceinline__ void stage2d_body(const KParams& P, const KBufs& B, i
         const double eb = T.v(EB, lo), bb1 = T.v(BB1, lo), bb2 = T.v(BB2, lo);
         const double ptb = (P.gamma - 1) * eb - 0.5 * (P.gamma - 2) * (bb1 * bb1 + bb2 * bb2);
         const double* v = T.V + d * RC;
-        double gv = d4(v, lo, d == 0 ? 1 : RX, rdl2);
+        double gv = o6d ? d6(v, lo, 1, rdl2) : d4(v, lo, d == 0 ? 1 : RX, rdl2);
         if (z) gv = 0;
         out[EN] -= dt * ptb * gv;
         const double bbd = d == 0 ? bb1 : bb2;
-        double g0 = d4(v, lo, 1, 0.5 * T.rd0[lxo]);
-        if ((P.bt[0] != 0) && zero3dn(gi, n0)) g0 = 0;
+        double g0 = dflux<O6>(v, lo, 1, 0.5 * T.rd0[lxo]);
+        if (((P.bt[0] != 0) && zero3dn(gi, n0)) || (O6 && edge6(gi, n0))) g0 = 0;
         out[EN] += dt * bb1 * bbd * g0;
         double g1 = d4(v, lo, RX, 0.5 * T.rd1[lyo]);
         if ((P.bt[1] != 0) && zero3dn(gj, n1)) g1 = 0;
@@ -614,26 +624,30 @@ __device__ __forceinline__ void stage2d_body(const KParams& P, const KBufs& B, i
   }
 }
 
-template <int MODE, bool BG, bool MIX>
+template <int MODE, bool BG, bool MIX, bool O6>
 __global__ void __launch_bounds__(NTHREADS, SMAUG_MINB2D) stage2d_fast(const KParams P, const KBufs B) {
-  stage2d_body<MODE, BG, MIX>(P, B, blockIdx.x, blockIdx.y);
+  stage2d_body<MODE, BG, MIX, O6>(P, B, blockIdx.x, blockIdx.y);
 }
 
-// launch helper: picks the background specialisation
-template <int MODE, bool MIX>
-static cudaError_t launch_stage2d(const KParams& K, const KBufs& B, cudaStream_t st) {
+// launch helper: picks the background and stencil-order specialisations
+template <int MODE, bool MIX, bool O6>
+static cudaError_t launch_stage2d_o(const KParams& K, const KBufs& B, cudaStream_t st) {
   dim3 block(TX, TY);
   dim3 grid((K.n0 - 4 + TX - 1) / TX, (K.n1 - 4 + TY - 1) / TY);
   if (K.has_bg) {
-    stage2d_fast<MODE, true, MIX><<<grid, block, s2::smem_bytes<true, MIX>(), st>>>(K, B);
+    stage2d_fast<MODE, true, MIX, O6><<<grid, block, s2::smem_bytes<true, MIX, O6>(), st>>>(K, B);
   } else {
-    stage2d_fast<MODE, false, MIX><<<grid, block, s2::smem_bytes<false, MIX>(), st>>>(K, B);
+    stage2d_fast<MODE, false, MIX, O6><<<grid, block, s2::smem_bytes<false, MIX, O6>(), st>>>(K, B);
   }
   return cudaGetLastError();
 }
+template <int MODE, bool MIX>
+static cudaError_t launch_stage2d(const KParams& K, const KBufs& B, cudaStream_t st) {
+  return K.order6 ? launch_stage2d_o<MODE, MIX, true>(K, B, st) : launch_stage2d_o<MODE, MIX, false>(K, B, st);
+}
 
-template <int MODE, bool BG, bool MIX>
+template <int MODE, bool BG, bool MIX, bool O6>
 static cudaError_t stage2d_attr() {
-  return cudaFuncSetAttribute(stage2d_fast<MODE, BG, MIX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)s2::smem_bytes<BG, MIX>());
+  return cudaFuncSetAttribute(stage2d_fast<MODE, BG, MIX, O6>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)s2::smem_bytes<BG, MIX, O6>());
 }

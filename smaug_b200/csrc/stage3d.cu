@@ -14,14 +14,19 @@ cudaError_t launch_stage3d_any(int mode, bool mix, const KParams& K, const KBufs
 
 cudaError_t stage3d_set_attributes() {
   cudaError_t e;
-  if ((e = stage3d_attr<SMAUG_INT_EULER, true, false>())) return e;
-  if ((e = stage3d_attr<SMAUG_INT_EULER, false, false>())) return e;
-  if ((e = stage3d_attr<SMAUG_INT_RK4, true, false>())) return e;
-  if ((e = stage3d_attr<SMAUG_INT_RK4, false, false>())) return e;
-  if ((e = stage3d_attr<SMAUG_INT_EULER, true, true>())) return e;
-  if ((e = stage3d_attr<SMAUG_INT_EULER, false, true>())) return e;
-  if ((e = stage3d_attr<SMAUG_INT_RK4, true, true>())) return e;
-  return stage3d_attr<SMAUG_INT_RK4, false, true>();
+#define SMAUG_ATTR3(M, BG, MIX)                                              \
+  if ((e = stage3d_attr<M, BG, MIX, false>())) return e;                   \
+  if ((e = stage3d_attr<M, BG, MIX, true>())) return e;
+  SMAUG_ATTR3(SMAUG_INT_EULER, true, false)
+  SMAUG_ATTR3(SMAUG_INT_EULER, false, false)
+  SMAUG_ATTR3(SMAUG_INT_RK4, true, false)
+  SMAUG_ATTR3(SMAUG_INT_RK4, false, false)
+  SMAUG_ATTR3(SMAUG_INT_EULER, true, true)
+  SMAUG_ATTR3(SMAUG_INT_EULER, false, true)
+  SMAUG_ATTR3(SMAUG_INT_RK4, true, true)
+  SMAUG_ATTR3(SMAUG_INT_RK4, false, true)
+#undef SMAUG_ATTR3
+  return cudaSuccess;
 }
 
 }  // namespace smaug

@@ -54,23 +54,26 @@ constexpr int BS1 = BX, BS2 = BX * BY;  // box strides
 __host__ __device__ constexpr int max3(int a, int b, int c) {
   return a > b ? (a > c ? a : c) : (b > c ? b : c);
 }
-constexpr int FA = max3((T0 + 4) * T1 * T2, T0 * (T1 + 4) * T2, T0 * T1 * (T2 + 4));
+// flux arrays: the tile +-2 (+-3 for the 6th-order derivative) along the direction
+template <bool O6>
+__host__ __device__ constexpr int fa() {
+  return max3((T0 + (O6 ? 6 : 4)) * T1 * T2, T0 * (T1 + (O6 ? 6 : 4)) * T2, T0 * T1 * (T2 + (O6 ? 6 : 4)));
+}
 constexpr int NA = max3(T0 * (T1 + 2) * (T2 + 2), (T0 + 2) * T1 * (T2 + 2), (T0 + 2) * (T1 + 2) * T2);
-constexpr int FLUX_SCR = 10 * FA;
 // ratio area: the nu area extended by one cell below along the direction
 constexpr int RA = max3((T0 + 1) * (T1 + 2) * (T2 + 2), (T0 + 2) * (T1 + 1) * (T2 + 2),
                         (T0 + 2) * (T1 + 2) * (T2 + 1));
 constexpr int HYP_SCR = BC + RA + 2 * NA;
 constexpr int NMET = 2 * (BX + BY + BZ);
-template <bool MIX>
+template <bool MIX, bool O6 = false>
 __host__ __device__ constexpr size_t union_bytes() {
-  return FLUX_SCR * sizeof(double) > HYP_SCR * sizeof(typename Form<MIX>::H)
-             ? FLUX_SCR * sizeof(double)
+  return 10 * fa<O6>() * sizeof(double) > HYP_SCR * sizeof(typename Form<MIX>::H)
+             ? 10 * fa<O6>() * sizeof(double)
              : HYP_SCR * sizeof(typename Form<MIX>::H);
 }
-template <bool MIX>
+template <bool MIX, bool O6 = false>
 __host__ __device__ constexpr size_t smem_bytes() {
-  return sizeof(double) * (BC + NMET) + union_bytes<MIX>() + sizeof(int) * BC;
+  return sizeof(double) * (BC + NMET) + union_bytes<MIX, O6>() + sizeof(int) * BC;
 }
 __host__ __device__ constexpr int tdim(int d) { return d == 0 ? T0 : (d == 1 ? T1 : T2); }
 __host__ __device__ constexpr int bstride(int d) { return d == 0 ? 1 : (d == 1 ? BS1 : BS2); }
@@ -362,14 +365,16 @@ __device__ __forceinline__ void flux3(const double* s, const double* g, double r
   v[2] = m[2] * r;
 }
 
-// flux phase along D: fluxes on the tile +-2 along D, divergence and the
-// background energy terms at the tile cells
-template <bool BG, bool MIX, int D>
+// flux phase along D: fluxes on the tile +-2 along D (+-3 for the 6th-order
+// derivative), divergence and the background energy terms at the tile cells
+template <bool BG, bool MIX, int D, bool O6>
 __device__ __forceinline__ void flux_pass3(const Box3& X, const KParams& P, const KBufs& B, int tid,
                                            bool active, const int* lt, const int* gt, double dt,
                                            const double* gc, double* out) {
-  constexpr int E0 = s3::T0 + (D == 0 ? 4 : 0), E1 = s3::T1 + (D == 1 ? 4 : 0), E2 = s3::T2 + (D == 2 ? 4 : 0);
-  constexpr int G0 = s3::H - (D == 0 ? 2 : 0), G1 = s3::H - (D == 1 ? 2 : 0), G2 = s3::H - (D == 2 ? 2 : 0);
+  constexpr int FH = O6 ? 3 : 2, FA = s3::fa<O6>();
+  constexpr int E0 = s3::T0 + (D == 0 ? 2 * FH : 0), E1 = s3::T1 + (D == 1 ? 2 * FH : 0);
+  constexpr int E2 = s3::T2 + (D == 2 ? 2 * FH : 0);
+  constexpr int G0 = s3::H - (D == 0 ? FH : 0), G1 = s3::H - (D == 1 ? FH : 0), G2 = s3::H - (D == 2 ? FH : 0);
   constexpr int NAREA = E0 * E1 * E2;
   constexpr int FS = D == 0 ? 1 : (D == 1 ? E0 : E0 * E1);
   using ST = typename Form<MIX>::S;
@@ -393,22 +398,22 @@ __device__ __forceinline__ void flux_pass3(const Box3& X, const KParams& P, cons
       flux3<BG, D>(s, g, X.R[(lz * s3::BY + ly) * s3::BX + lx], P.gamma, f, v);
     }
 #pragma unroll
-    for (int k = 0; k < 7; k++) F[k * s3::FA + r] = f[k];
+    for (int k = 0; k < 7; k++) F[k * FA + r] = f[k];
     if (BG) {
 #pragma unroll
-      for (int k = 0; k < 3; k++) F[(7 + k) * s3::FA + r] = v[k];
+      for (int k = 0; k < 3; k++) F[(7 + k) * FA + r] = v[k];
     }
   }
   __syncthreads();
   if (active) {
-    const bool z = (P.bt[D] != 0) && zero3dn(gt[D], n[D]);
+    const bool z = ((P.bt[D] != 0) && zero3dn(gt[D], n[D])) || (O6 && edge6(gt[D], n[D]));
     const double rdl2 = 0.5 * X.rd[D][lt[D]];
     const int fo = ((lt[2] - G2) * E1 + (lt[1] - G1)) * E0 + (lt[0] - G0);
     constexpr int c1 = D == 0 ? 1 : 0, c2 = D == 2 ? 1 : 2;
     const int fld[7] = {R3, M3, M3 + 1, M3 + 2, E3, B3 + c1, B3 + c2};
 #pragma unroll
     for (int k = 0; k < 7; k++) {
-      double gk = d4(F + k * s3::FA, fo, FS, rdl2);
+      double gk = dflux<O6>(F + k * FA, fo, FS, rdl2);
       if (z) gk = 0;
       out[fld[k]] = out[fld[k]] - dt * gk;
     }
@@ -417,12 +422,12 @@ __device__ __forceinline__ void flux_pass3(const Box3& X, const KParams& P, cons
       // the derivative-along-D part of sum_i Bb_i Bb_d dv_d/dx_i
       const double bb[3] = {gc[2], gc[3], gc[4]};
       const double ptb = (P.gamma - 1) * gc[0] - 0.5 * (P.gamma - 2) * (bb[0] * bb[0] + bb[1] * bb[1] + bb[2] * bb[2]);
-      double gv = d4(F + (7 + D) * s3::FA, fo, FS, rdl2);
+      double gv = dflux<O6>(F + (7 + D) * FA, fo, FS, rdl2);
       if (z) gv = 0;
       out[E3] -= dt * ptb * gv;
 #pragma unroll
       for (int k = 0; k < 3; k++) {
-        double gk = d4(F + (7 + k) * s3::FA, fo, FS, rdl2);
+        double gk = dflux<O6>(F + (7 + k) * FA, fo, FS, rdl2);
         if (z) gk = 0;
         out[E3] += dt * bb[D] * bb[k] * gk;
       }
@@ -431,7 +436,7 @@ __device__ __forceinline__ void flux_pass3(const Box3& X, const KParams& P, cons
   __syncthreads();
 }
 
-template <int MODE, bool BG, bool MIX>
+template <int MODE, bool BG, bool MIX, bool O6>
 __global__ void __launch_bounds__(s3::NT, SMAUG_MINB3D) stage3d_fast(const KParams P, const KBufs B) {
   using ST = typename Form<MIX>::S;
   const ST* u = static_cast<const ST*>(B.uin);
@@ -445,7 +450,7 @@ __global__ void __launch_bounds__(s3::NT, SMAUG_MINB3D) stage3d_fast(const KPara
   X.rd[1] = X.rd[0] + s3::BX;
   X.rd[2] = X.rd[1] + s3::BY;
   X.U = X.rd[2] + s3::BZ;
-  X.C = reinterpret_cast<int*>(reinterpret_cast<unsigned char*>(X.U) + s3::union_bytes<MIX>());
+  X.C = reinterpret_cast<int*>(reinterpret_cast<unsigned char*>(X.U) + s3::union_bytes<MIX, O6>());
   const int tid = threadIdx.x;
   const int tx = tid % s3::T0, ty = (tid / s3::T0) % s3::T1, tz = tid / (s3::T0 * s3::T1);
   const int n[3] = {P.n0, P.n1, P.n2};
@@ -519,9 +524,9 @@ __global__ void __launch_bounds__(s3::NT, SMAUG_MINB3D) stage3d_fast(const KPara
   }
 
   // ---- fluxes and divergence, direction 0, 1, 2 ----------------------------
-  flux_pass3<BG, MIX, 0>(X, P, B, tid, active, lt, gt, dt, gc, out);
-  flux_pass3<BG, MIX, 1>(X, P, B, tid, active, lt, gt, dt, gc, out);
-  flux_pass3<BG, MIX, 2>(X, P, B, tid, active, lt, gt, dt, gc, out);
+  flux_pass3<BG, MIX, 0, O6>(X, P, B, tid, active, lt, gt, dt, gc, out);
+  flux_pass3<BG, MIX, 1, O6>(X, P, B, tid, active, lt, gt, dt, gc, out);
+  flux_pass3<BG, MIX, 2, O6>(X, P, B, tid, active, lt, gt, dt, gc, out);
 
   // ---- gravity (addgrav_cd2, src/centdiff2.cu:118-154) --------------------
   if (P.has_grav && active) {
@@ -657,19 +662,23 @@ __global__ void __launch_bounds__(s3::NT, SMAUG_MINB3D) stage3d_fast(const KPara
   }
 }
 
-template <int MODE, bool MIX>
-static cudaError_t launch_stage3d(const KParams& K, const KBufs& B, cudaStream_t st) {
+template <int MODE, bool MIX, bool O6>
+static cudaError_t launch_stage3d_o(const KParams& K, const KBufs& B, cudaStream_t st) {
   dim3 grid((K.n0 - 4 + s3::T0 - 1) / s3::T0, (K.n1 - 4 + s3::T1 - 1) / s3::T1,
             (K.n2 - 4 + s3::T2 - 1) / s3::T2);
   if (K.has_bg)
-    stage3d_fast<MODE, true, MIX><<<grid, s3::NT, s3::smem_bytes<MIX>(), st>>>(K, B);
+    stage3d_fast<MODE, true, MIX, O6><<<grid, s3::NT, s3::smem_bytes<MIX, O6>(), st>>>(K, B);
   else
-    stage3d_fast<MODE, false, MIX><<<grid, s3::NT, s3::smem_bytes<MIX>(), st>>>(K, B);
+    stage3d_fast<MODE, false, MIX, O6><<<grid, s3::NT, s3::smem_bytes<MIX, O6>(), st>>>(K, B);
   return cudaGetLastError();
 }
+template <int MODE, bool MIX>
+static cudaError_t launch_stage3d(const KParams& K, const KBufs& B, cudaStream_t st) {
+  return K.order6 ? launch_stage3d_o<MODE, MIX, true>(K, B, st) : launch_stage3d_o<MODE, MIX, false>(K, B, st);
+}
 
-template <int MODE, bool BG, bool MIX>
+template <int MODE, bool BG, bool MIX, bool O6>
 static cudaError_t stage3d_attr() {
-  return cudaFuncSetAttribute(stage3d_fast<MODE, BG, MIX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)s3::smem_bytes<MIX>());
+  return cudaFuncSetAttribute(stage3d_fast<MODE, BG, MIX, O6>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)s3::smem_bytes<MIX, O6>());
 }

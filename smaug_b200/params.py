@@ -42,7 +42,8 @@ class SmaugParams(ctypes.Structure):
         ("pad_model", ctypes.c_int32),
         ("boundtype", (ctypes.c_int32 * 2) * 3),
         ("driver", ctypes.c_int32),
-        ("reserved_i", ctypes.c_int32 * 7),
+        ("stencil_order", ctypes.c_int32),
+        ("reserved_i", ctypes.c_int32 * 6),
         ("dx", ctypes.c_double * 3),
         ("dt", ctypes.c_double),
         ("dtmax", ctypes.c_double),
@@ -111,10 +112,12 @@ def make_params(ndim=2, n=(132, 132, 1), dx=None, gamma=5.0 / 3.0, courant=0.3,
                 boundtype=None, integrator=INT_EULER, g=(0.0, 0.0, 0.0),
                 eta=0.0, xmin=(0.0, 0.0, 0.0), pad_model=PAD_STRAY,
                 driver=DRIVER_NONE, drv_amp=0.0, drv_period=0.0, precision=PREC_FP64,
-                drv_x0=(0.0, 0.0, 0.0), drv_sigma=(0.0, 0.0, 0.0)):
+                drv_x0=(0.0, 0.0, 0.0), drv_sigma=(0.0, 0.0, 0.0), stencil_order=4):
     """Build a parameter block.  Defaults: the reference's Orszag-Tang model
     (models/iosmaugparams.h.ot) with a 0.3 Courant number; `chyp` may be a
-    scalar (every field) or a sequence indexed by field."""
+    scalar (every field) or a sequence indexed by field; stencil_order 6
+    selects the 6th-order flux derivative of the reference's USE_DORDER3
+    build."""
     p = SmaugParams()
     p.version = PARAMS_VERSION
     p.ndim = ndim
@@ -154,6 +157,7 @@ def make_params(ndim=2, n=(132, 132, 1), dx=None, gamma=5.0 / 3.0, courant=0.3,
         else:
             p.boundtype[d][0] = p.boundtype[d][1] = bt
     p.driver = driver
+    p.stencil_order = stencil_order
     p.drv_amp = drv_amp
     p.drv_period = drv_period
     return p

@@ -32,6 +32,10 @@ fields, DT 1, courant 0.3, chyp 0.2, PGAMMA 1.66666667):
   t3s      4x4x4 interior (8^3 = 512 cells: one thread block), 20 steps
   t3a      12x12x8 interior (16x16x12 = 6 blocks), steps 0-5 and 10
   t3b      20x12x8 interior (24x16x12 = 9 blocks), steps 0-3
+6th-order flux derivative (the reference built with -DUSE_DORDER3,
+src/gradops.cu:450-453; one thread block each):
+  d16      2D, as g16 with seed 15, 20 steps
+  d3s      3D, as t3s with seed 25, 20 steps
 Every 3D grid holds a whole number of 512-thread blocks: the reference's
 contcd4 ghost kernels (models/boundary.cu.fluxtube1:16-85) have no
 cell-count guard, so a partial last block would write past the state array.
@@ -82,6 +86,12 @@ CASES3 = {
 }
 
 
+# the reference built with -DUSE_DORDER3 (same tuple layouts as CASES / CASES3)
+CASES_O6 = {"d16": (16, 16, 15, 21, [1, 2, 3, 5, 10, 20])}
+CASES3_O6 = {"d3s": ((4, 4, 4), 25, 21, [1, 2, 3, 5, 10, 20], 1)}
+O6 = ("USE_DORDER3",)
+
+
 def tube_state(nx, ny, nz, seed, gamma=GAMMA_REF):
     """Smooth 3D state with nonzero backgrounds on [0, L3]^3: stratified-like
     rho_b, p_b along dim 0, a uniform-plus-sinusoid background field, and
@@ -117,13 +127,13 @@ def tube_state(nx, ny, nz, seed, gamma=GAMMA_REF):
     return w, np.stack([X, Y, Z])
 
 
-def _build3(name, nx, ny, nz, nt, bt_ref=None):
+def _build3(name, nx, ny, nz, nt, bt_ref=None, defines=()):
     from oracle import build_ref
     extra = {}
     for d, t in enumerate(bt_ref or ()):
         extra["BCU%d" % d] = str(t)
         extra["BCL%d" % d] = str(t)
-    return build_ref.build_ref(name, nx, ny, nt, nk=nz, verbose=False,
+    return build_ref.build_ref(name, nx, ny, nt, nk=nz, verbose=False, defines=defines,
                                XMIN="0.0", XMAX=repr(L3), YMIN="0.0", YMAX=repr(L3),
                                ZMIN="0.0", ZMAX=repr(L3), PGRAV0=repr(G3), PGRAV1="0.0",
                                PGRAV2="0.0", **extra)
@@ -156,19 +166,21 @@ def prepare():
     from smaug_b200 import formats
     from oracle import build_ref
     os.makedirs(WORK, exist_ok=True)
-    for name, case in _selected(CASES).items():
-        nx, ny, seed, nt, keep = case[:5]
-        w, pos = ot_state(nx, ny, seed)
-        formats.write_ini(os.path.join(WORK, name + ".ini"), w, pos)
-        build_ref.build_ref(name, nx, ny, nt, verbose=False, **_bc_defines(case))
-        print("prepared", name)
-    for name, case in _selected(CASES3).items():
-        (nx, ny, nz), seed, nt, keep, runs = case[:5]
-        w, pos = tube_state(nx, ny, nz, seed)
-        formats.write_ini(os.path.join(WORK, name + ".ini"), w, pos, gamma=GAMMA_REF,
-                          g=(G3, 0.0, 0.0))
-        _build3(name, nx, ny, nz, nt, case[5] if len(case) > 5 else None)
-        print("prepared", name)
+    for table, defines in ((CASES, ()), (CASES_O6, O6)):
+        for name, case in _selected(table).items():
+            nx, ny, seed, nt, keep = case[:5]
+            w, pos = ot_state(nx, ny, seed)
+            formats.write_ini(os.path.join(WORK, name + ".ini"), w, pos)
+            build_ref.build_ref(name, nx, ny, nt, verbose=False, defines=defines, **_bc_defines(case))
+            print("prepared", name)
+    for table, defines in ((CASES3, ()), (CASES3_O6, O6)):
+        for name, case in _selected(table).items():
+            (nx, ny, nz), seed, nt, keep, runs = case[:5]
+            w, pos = tube_state(nx, ny, nz, seed)
+            formats.write_ini(os.path.join(WORK, name + ".ini"), w, pos, gamma=GAMMA_REF,
+                              g=(G3, 0.0, 0.0))
+            _build3(name, nx, ny, nz, nt, case[5] if len(case) > 5 else None, defines)
+            print("prepared", name)
 
 
 def _run_one(name, keep, tag=""):
@@ -196,11 +208,11 @@ def _bc_defines(case):
 
 
 def run():
-    for name, case in _selected(CASES).items():
+    for name, case in _selected({**CASES, **CASES_O6}).items():
         _run_one(name, case[4])
         if name in TWICE:
             _run_one(name, case[4], "_r1")
-    for name, case in _selected(CASES3).items():
+    for name, case in _selected({**CASES3, **CASES3_O6}).items():
         keep, runs = case[3], case[4]
         for r in range(runs):
             _run_one(name, keep, "" if r == 0 else "_r%d" % r)
@@ -208,9 +220,11 @@ def run():
 
 def collect():
     from smaug_b200 import formats
-    for name, case in _selected(CASES3).items():
+    for name, case in _selected({**CASES3, **CASES3_O6}).items():
         (nx, ny, nz), seed, nt, keep, runs = case[:5]
         extra = {"bt": np.array(case[6]), "bt_ref": np.array(case[5])} if len(case) > 6 else {}
+        if name in CASES3_O6:
+            extra["order"] = 6
         w0, pos0, _ = formats.read_ini(os.path.join(WORK, name + ".ini"), 3)
         states, times = [], []
         for k in keep:
@@ -223,7 +237,7 @@ def collect():
                             dx=np.array([L3 / nx, L3 / ny, L3 / nz]),
                             g=np.array([G3, 0.0, 0.0]), **extra)
         print("wrote", name)
-    for name, case in _selected(CASES).items():
+    for name, case in _selected({**CASES, **CASES_O6}).items():
         nx, ny, seed, nt, keep = case[:5]
         bt = case[5] if len(case) > 5 else (0, 0)
         w0, pos0, _ = formats.read_ini(os.path.join(WORK, name + ".ini"), 2)
@@ -232,7 +246,7 @@ def collect():
             w, pos, h = formats.read_out(os.path.join(RUNS, name, "out", "ref_%d.out" % k))
             states.append(w[:6])
             times.append(h["t"])
-        extra = {}
+        extra = {"order": 6} if name in CASES_O6 else {}
         # the last saved state of a second run of the same binary (name_r1)
         if os.path.isdir(os.path.join(RUNS, name + "_r1")):
             extra["last_r1"] = formats.read_out(

@@ -11,6 +11,8 @@ BOUNDARY = ("f16x", "f18y")            # fixed ghosts along dim 0 / dim 1
 ONESTEP = ("ot24x20",)                 # consecutive steps, one-step parity
 RACE = ("ot128",)                      # 128^2, 200 steps, two runs of the reference
 STRICT3 = ("t3s", "t3a", "t3b", "t3f")  # 3D flux-tube build, contcd4 (t3f: fixed dim 0) ghosts
+ORDER6 = ("d16",)                      # 2D, the reference built with -DUSE_DORDER3
+ORDER6_3D = ("d3s",)                   # 3D, the same
 
 
 def load(name):
@@ -27,6 +29,8 @@ def load(name):
 
 def params(d, **kw):
     kw.setdefault("integrator", P.INT_EULER)
+    if "order" in d:
+        kw.setdefault("stencil_order", int(d["order"]))
     if d["w0"].ndim == 4:
         nz, ny, nx = d["w0"].shape[1:]
         bt = [int(b) for b in d["bt"]] if "bt" in d else [P.BC_CONTCD4] * 3

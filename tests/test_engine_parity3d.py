@@ -99,7 +99,7 @@ def test_larger_grid3d_against_oracle(engine_lib, oracle):
     assert_parity(got, ref)
 
 
-@pytest.mark.parametrize("name", G.STRICT3)
+@pytest.mark.parametrize("name", G.STRICT3 + G.ORDER6_3D)
 def test_engine_matches_reference_run_3d(engine_lib, name):
     """Every field at every saved step of the reference's 3D build."""
     d = G.load(name)

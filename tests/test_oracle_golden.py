@@ -13,7 +13,7 @@ from tests.util import rel_l2
 TOL = 1e-13
 
 
-@pytest.mark.parametrize("name", G.STRICT + G.BOUNDARY)
+@pytest.mark.parametrize("name", G.STRICT + G.BOUNDARY + G.ORDER6)
 def test_oracle_matches_reference_run(oracle, name):
     d = G.load(name)
     p = G.params(d)
@@ -47,7 +47,7 @@ def test_oracle_one_step_multiblock(oracle, name):
             assert err <= TOL, (name, steps[b], f, err)
 
 
-@pytest.mark.parametrize("name", G.STRICT3)
+@pytest.mark.parametrize("name", G.STRICT3 + G.ORDER6_3D)
 def test_oracle_matches_reference_run_3d(oracle, name):
     """3D: every one of the 13 fields (backgrounds included) at every saved
     step of the reference's flux-tube build (-DUSE_SAC_3D, contcd4 ghosts in
