@@ -473,6 +473,57 @@ def _adjoint_case(args, sa, q, p, u0, pos, rhob, theta0, shift, obs_z, nsteps, r
     return line
 
 
+def snapshots_main(args):
+    """--workload snapshots: RK4 steps of a 1024^2 Orszag-Tang grid with a
+    reference .out snapshot every 10 steps (the driver's cfgsavefrequency
+    output, src/iosmaug.c:509-517), written synchronously (smaug_write_out)
+    and asynchronously (smaug_write_out_async: copy queued on the stream,
+    file written by a host thread while the engine steps).  Host wall clock
+    over the whole loop, files included; value = the asynchronous steps/s."""
+    import shutil
+    import tempfile
+    import torch
+    from smaug_b200 import engine
+    n = args.n if args.n is not None and args.n != WORKLOAD_N else 1024
+    nsteps, every = 60, 10
+    p, w, pos = make_case(n, 1, 0)
+    out = tempfile.mkdtemp(prefix="smaug_snap_")
+    res = {}
+    try:
+        for mode in ("sync", "async", "none"):
+            e = engine.Engine(p, w, pos)
+            e.step(args.warmup)
+            t0 = time.perf_counter()
+            for k in range(nsteps // every):
+                e.step_async(every)
+                path = os.path.join(out, "%s_%d.out" % (mode, k))
+                if mode == "sync":
+                    e.write_out(path, it=k, t=0.0)
+                elif mode == "async":
+                    e.write_out_async(path, it=k, t=0.0)
+            if mode == "async":
+                e.wait_writes()
+            e.sync()
+            torch.cuda.synchronize()
+            res[mode] = time.perf_counter() - t0
+            e.close()
+        same = all(open(os.path.join(out, "sync_%d.out" % k), "rb").read() ==
+                   open(os.path.join(out, "async_%d.out" % k), "rb").read() for k in range(nsteps // every))
+        size = os.path.getsize(os.path.join(out, "sync_0.out"))
+    finally:
+        shutil.rmtree(out, ignore_errors=True)
+    line = {"metric": "RK4 steps/s with a .out snapshot every %d steps" % every,
+            "value": nsteps / res["async"], "unit": "steps/s", "n_gpus": 1, "steps": nsteps,
+            "warmup": args.warmup, "ms_per_step": res["async"] / nsteps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "2D Orszag-Tang %dx%d, FP64 RK4, snapshot every %d steps" % (n, n, every),
+                       "timing": "host wall clock over the loop, files written and closed"},
+            "sync_steps_per_s": nsteps / res["sync"], "no_output_steps_per_s": nsteps / res["none"],
+            "speedup_vs_sync": res["sync"] / res["async"], "bytes_per_snapshot": size,
+            "files_identical": bool(same)}
+    print(json.dumps(line), flush=True)
+
+
 def max_over_ranks(ms, ws, device="cuda"):
     """The slowest rank's time: every rank takes part (the same collective in
     the same order on every rank); one rank returns its own value."""
@@ -582,7 +633,7 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="ot", choices=["ot", "tube", "ensemble", "adjoint"])
+    ap.add_argument("--workload", default="ot", choices=["ot", "tube", "ensemble", "adjoint", "snapshots"])
     ap.add_argument("--adj-steps", type=int, default=400)
     ap.add_argument("--obs-z", type=float, default=3.0e6,
                     help="height of the observed v_z row for --workload adjoint [m]")
@@ -612,6 +663,9 @@ def main():
         return
     if args.workload == "adjoint" and args.impl != "reference":
         adjoint_main(args)
+        return
+    if args.workload == "snapshots" and args.impl != "reference":
+        snapshots_main(args)
         return
     if args.impl == "reference":
         reference_arm(args, ws, rank)

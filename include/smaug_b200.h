@@ -176,6 +176,21 @@ int smaug_get_cmax(smaug_handle_t h, double* cmax);
 int smaug_write_out(smaug_handle_t h, const char* path, const char* name,
                     int32_t it, double t);
 
+/* Asynchronous snapshot (the reference writes .out files synchronously from
+   the step loop, src/iosmaug.c:509-517 writevacconfig): enqueue the copy of
+   the current state on the engine's stream into a pinned host buffer and
+   return; a host thread writes the .out file when the copy has completed,
+   while the caller keeps stepping.  Two buffers are used in turn, so a third
+   call first waits for the oldest write.  Errors of the write itself are
+   reported by smaug_wait_writes. */
+int smaug_write_out_async(smaug_handle_t h, const char* path, const char* name,
+                          int32_t it, double t);
+
+/* Wait for every pending asynchronous write; returns the first write error
+   since the last call (SMAUG_E_IO with the file's message), else 0.
+   smaug_destroy waits as well. */
+int smaug_wait_writes(smaug_handle_t h);
+
 /* Release all device memory of the handle. */
 int smaug_destroy(smaug_handle_t h);
 

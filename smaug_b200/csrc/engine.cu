@@ -27,6 +27,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/smaug_b200.h"
@@ -143,6 +144,17 @@ __global__ void cmax2d_kernel(const KParams P, const double* u, const double* bg
 // ---------------------------------------------------------------------------
 // host engine
 // ---------------------------------------------------------------------------
+// One pending asynchronous .out write: the state is copied on the engine's
+// stream into a pinned host buffer, and a host thread writes the file once the
+// copy's event has completed.
+struct Snapshot {
+  double* host = nullptr;        // pinned, nvar * ncell doubles (allocated on first use)
+  cudaEvent_t ready = nullptr;   // recorded after the device-to-host copies
+  std::thread worker;
+  int rc = SMAUG_OK;             // result of the write, read after the join
+  std::string err;
+};
+
 struct Engine {
   smaug_params_t P{};
   KParams K{};
@@ -169,10 +181,30 @@ struct Engine {
   int64_t it = 0;
   int device = 0;
   cudaStream_t own_stream = nullptr;     // created by the engine
+  Snapshot snap[2];                      // asynchronous .out writes, used in turn
+  int snap_next = 0;
+  int snap_rc = SMAUG_OK;                // first failed write since the last wait
+  std::string snap_err;
 };
+
+// wait for the write of slot s (if any) and keep its error
+static void join_snapshot(Engine* e, Snapshot& s) {
+  if (!s.worker.joinable()) return;
+  s.worker.join();
+  if (s.rc != SMAUG_OK && e->snap_rc == SMAUG_OK) {
+    e->snap_rc = s.rc;
+    e->snap_err = s.err;
+  }
+  s.rc = SMAUG_OK;
+}
 
 static void free_engine(Engine* e) {
   if (!e) return;
+  for (Snapshot& s : e->snap) {
+    join_snapshot(e, s);
+    if (s.host) cudaFreeHost(s.host);
+    if (s.ready) cudaEventDestroy(s.ready);
+  }
   for (int i = 0; i < 3; i++) {
     cudaFree(e->d_u[i]);
     cudaFree(e->d_h[i]);
@@ -799,6 +831,61 @@ extern "C" int smaug_write_out(smaug_handle_t h, const char* path, const char* n
   int rc = smaug_get_state(h, w.data());
   if (rc) return rc;
   return smaug::write_out_host(path, &e->P, w.data(), e->pos_host.data(), name, it, t);
+}
+
+// Asynchronous .out snapshot: enqueue the copies on the engine's stream and
+// return; a host thread writes the file when they complete.  Two slots are
+// used in turn, so a third call waits for the write of the first.
+extern "C" int smaug_write_out_async(smaug_handle_t h, const char* path, const char* name, int32_t it,
+                                     double t) {
+  smaug::clear_error();
+  if (!h || !path) return smaug::set_error(SMAUG_E_INVALID, "null argument");
+  Engine* e = H(h);
+  smaug::Snapshot& s = e->snap[e->snap_next];
+  smaug::join_snapshot(e, s);
+  const size_t nc = (size_t)e->ncell;
+  const size_t nvar = (size_t)(e->nevo + e->nbg);
+  if (!s.host) {
+    if (cudaMallocHost(&s.host, sizeof(double) * nvar * nc) != cudaSuccess) {
+      cudaGetLastError();
+      s.host = nullptr;
+      return smaug::set_error(SMAUG_E_NOMEM, "pinned snapshot buffer of %zu bytes", sizeof(double) * nvar * nc);
+    }
+  }
+  if (!s.ready) CUDA_TRY(cudaEventCreateWithFlags(&s.ready, cudaEventDisableTiming));
+  double* u = nullptr;
+  int rc = smaug::current_fp64(e, &u);
+  if (rc) return rc;
+  CUDA_TRY(cudaMemcpyAsync(s.host, u, sizeof(double) * e->nevo * nc, cudaMemcpyDeviceToHost, e->stream));
+  CUDA_TRY(cudaMemcpyAsync(s.host + (size_t)e->nevo * nc, e->d_bg, sizeof(double) * e->nbg * nc,
+                           cudaMemcpyDeviceToHost, e->stream));
+  CUDA_TRY(cudaEventRecord(s.ready, e->stream));
+  std::string spath(path), sname(name ? name : "");
+  const smaug_params_t P = e->P;
+  const double* pos = e->pos_host.data();
+  smaug::Snapshot* sp = &s;
+  s.worker = std::thread([sp, spath, sname, P, pos, it, t]() {
+    if (cudaEventSynchronize(sp->ready) != cudaSuccess) {
+      sp->rc = SMAUG_E_CUDA;
+      sp->err = std::string("snapshot copy: ") + cudaGetErrorString(cudaGetLastError());
+      return;
+    }
+    sp->rc = smaug::write_out_host(spath.c_str(), &P, sp->host, pos, sname.c_str(), it, t);
+    if (sp->rc != SMAUG_OK) sp->err = smaug::last_error();
+  });
+  e->snap_next ^= 1;
+  return SMAUG_OK;
+}
+
+extern "C" int smaug_wait_writes(smaug_handle_t h) {
+  smaug::clear_error();
+  if (!h) return smaug::set_error(SMAUG_E_INVALID, "null argument");
+  Engine* e = H(h);
+  for (smaug::Snapshot& s : e->snap) smaug::join_snapshot(e, s);
+  const int rc = e->snap_rc;
+  e->snap_rc = SMAUG_OK;
+  if (rc != SMAUG_OK) return smaug::set_error(rc, "%s", e->snap_err.c_str());
+  return SMAUG_OK;
 }
 
 extern "C" int smaug_destroy(smaug_handle_t h) {

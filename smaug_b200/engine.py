@@ -25,7 +25,7 @@ EXPORTS = [
     "smaug_batch_destroy", "smaug_batch_step_async", "smaug_batch_sync", "smaug_batch_set_stream",
     "smaug_adj_create", "smaug_adj_set_driver", "smaug_adj_forward", "smaug_adj_backward",
     "smaug_adj_tape_reserve", "smaug_adj_forward_tape", "smaug_adj_backward_tape",
-    "smaug_adj_destroy",
+    "smaug_adj_destroy", "smaug_write_out_async", "smaug_wait_writes",
 ]
 
 ERRORS = {1: "invalid", 2: "cuda", 3: "nomem", 4: "io", 5: "format", 6: "unsupported",
@@ -65,6 +65,9 @@ def lib():
         L.smaug_get_cmax.argtypes = [vp, dp]
         L.smaug_write_out.argtypes = [vp, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int32,
                                       ctypes.c_double]
+        L.smaug_write_out_async.argtypes = [vp, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int32,
+                                            ctypes.c_double]
+        L.smaug_wait_writes.argtypes = [vp]
         L.smaug_destroy.argtypes = [vp]
         L.smaug_last_error.restype = ctypes.c_char_p
         L.smaug_version.restype = ctypes.c_char_p
@@ -206,6 +209,20 @@ class Engine:
         i, tt, _ = self.time()
         _check(lib().smaug_write_out(self.h, path.encode(), name.encode(),
                                      int(i if it is None else it), float(tt if t is None else t)))
+
+    def write_out_async(self, path, name="test1", it=None, t=None):
+        """Snapshot the current state to a .out file without waiting: the copy
+        is queued on the engine's stream and a host thread writes the file
+        (errors surface in wait_writes)."""
+        if it is None or t is None:   # smaug_get_time waits for the engine's stream
+            i, tt, _ = self.time()
+            it = i if it is None else it
+            t = tt if t is None else t
+        _check(lib().smaug_write_out_async(self.h, path.encode(), name.encode(), int(it), float(t)))
+
+    def wait_writes(self):
+        """Wait for the pending write_out_async files; raises the first write error."""
+        _check(lib().smaug_wait_writes(self.h))
 
     def close(self):
         if getattr(self, "h", None):
