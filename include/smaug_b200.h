@@ -251,6 +251,17 @@ int smaug_adj_forward_tape(smaug_adj_t a, const double* u, double* u_next, doubl
 /* smaug_adj_backward of the step taped in `slot` (same t) */
 int smaug_adj_backward_tape(smaug_adj_t a, int32_t slot, const double* ubar_next, double* ubar,
                             double* thbar, double t, void* stream);
+
+/* The step adjoints of taped slots slot_lo .. slot_lo+nsteps-1 in reverse
+   order in one call, for the steps n_lo .. n_lo+nsteps-1 of a rollout (step
+   n at time t0 + n*dt).  ubar: in, the adjoint of the state after the last
+   step; out, the adjoint of the state before the first.  Before the adjoint
+   of step n_lo+k, gsteps[k] (6*ncell doubles, e.g. the gradient of a loss
+   term at that step's output) is added to it, when gsteps is not NULL.
+   thbar (3 doubles) accumulates the parameter adjoints (not cleared). */
+int smaug_adj_backward_tape_range(smaug_adj_t a, int32_t slot_lo, int32_t nsteps,
+                                  const double* gsteps, double* ubar, double* thbar,
+                                  double t0, int32_t n_lo, void* stream);
 int smaug_adj_destroy(smaug_adj_t a);
 
 /* Message of the calling thread's last failure ("" if none). */

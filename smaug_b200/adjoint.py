@@ -81,6 +81,18 @@ class StepAdjoint:
             float(t), ctypes.c_void_p(st)))
         return ubar, thbar
 
+    def backward_tape_range(self, slot_lo, nsteps, gsteps, ubar, thbar, t0, n_lo):
+        """The step adjoints of slots slot_lo .. slot_lo+nsteps-1 in reverse
+        order in one call (steps n_lo.. at t0 + n*dt): ubar is updated in
+        place from the adjoint after the last step to the adjoint before the
+        first, gsteps[k] (or nothing when None) is added before step k's
+        adjoint, thbar accumulates."""
+        st = torch.cuda.current_stream(ubar.device).cuda_stream
+        gp = None if gsteps is None else self._ptr(gsteps)
+        _engine._check(_engine.lib().smaug_adj_backward_tape_range(
+            self.h, int(slot_lo), int(nsteps), gp, self._ptr(ubar), self._ptr(thbar), float(t0),
+            int(n_lo), ctypes.c_void_p(st)))
+
     def close(self):
         if getattr(self, "h", None):
             _engine.lib().smaug_adj_destroy(self.h)
@@ -183,12 +195,12 @@ class _Rollout(torch.autograd.Function):
                     for n in range(s, e):
                         states.append(sa.forward_tape(states[-1], t0 + n * dt, n - s))
             grads = _Rollout._loss_grads(ctx.loss_fn, states, s)
-            for n in range(e - 1, s - 1, -1):
-                gl = grads[n - s]
-                g = gl * gL if gl is not None else torch.zeros_like(states[n - s + 1])
-                ubar = g if ubar is None else ubar + g
-                ubar, tb = sa.backward_tape(n - base, ubar, t0 + n * dt)
-                thbar = thbar + tb
+            gsteps = torch.stack([g if g is not None else torch.zeros_like(states[0]) for g in grads])
+            gsteps.mul_(gL)
+            if ubar is None:
+                ubar = torch.zeros_like(states[0])
+            # the segment's step adjoints in one call (gsteps[k] joins before step s+k)
+            sa.backward_tape_range(s - base, e - s, gsteps, ubar, thbar, t0, s)
         ctx.states = None
         dtype, device = ctx.theta_meta
         # ubar and thbar already carry the factor gL (it scales every loss gradient)

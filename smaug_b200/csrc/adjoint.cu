@@ -1032,6 +1032,7 @@ struct Adjoint {
   int* arg = nullptr;                  // [4][2] their cells
   double* tape = nullptr;              // [nslots][4][6][nc] stage inputs of taped steps
   int nslots = 0;
+  double* ubar2 = nullptr;             // [6][nc] second adjoint buffer of the range backward
 };
 
 static void free_adj(Adjoint* a) {
@@ -1055,6 +1056,7 @@ static void free_adj(Adjoint* a) {
   cudaFree(a->mx);
   cudaFree(a->arg);
   cudaFree(a->tape);
+  cudaFree(a->ubar2);
   delete a;
 }
 
@@ -1222,7 +1224,7 @@ static int adj_fwd(Adjoint* a, const double* u, double t, cudaStream_t st, doubl
 // The adjoint of one step from u.  Xs: the step's stage inputs from a tape
 // slot, or null to recompute them from u.
 static int adj_bwd(Adjoint* a, const double* u, const double* ubar_next, double* ubar, double* thbar,
-                   double t, cudaStream_t st, double* const* Xs) {
+                   double t, cudaStream_t st, double* const* Xs, bool thbar_accumulate = false) {
   if (!Xs) {
     int rc = adj_fwd(a, u, t, st, a->X);
     if (rc) return rc;
@@ -1239,7 +1241,7 @@ static int adj_bwd(Adjoint* a, const double* u, const double* ubar_next, double*
   const double half[4] = {0.0, 0.5, 0.5, 1.0};   // X_s = U + half[s] k_{s-1}
   // W = G^T ubar_next; ubar = W; k-bar of stage 4 = W / 6
   adj_head<<<G_LAUNCH(nc)>>>(a->K, ubar_next, a->W, ubar, a->Kb, wk[3]);
-  CUDA_TRY(cudaMemsetAsync(thbar, 0, sizeof(double) * 3, st));
+  if (!thbar_accumulate) CUDA_TRY(cudaMemsetAsync(thbar, 0, sizeof(double) * 3, st));
   const double dt = a->P.dt;
   const double ts[4] = {t, t + 0.5 * dt, t + 0.5 * dt, t + dt};
   const size_t eb = sizeof(double) * 6 * nc;
@@ -1269,6 +1271,12 @@ static int adj_bwd(Adjoint* a, const double* u, const double* ubar_next, double*
     CUDA_TRY(cudaGetLastError());
   }
   return SMAUG_OK;
+}
+
+// y += x over n doubles
+__global__ void add_inplace(double* y, const double* x, long n) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i < n) y[i] += x[i];
 }
 
 // stage-input pointers of tape slot `slot`
@@ -1358,6 +1366,35 @@ extern "C" int smaug_adj_backward_tape(smaug_adj_t h, int32_t slot, const double
   int rc = smaug::tape_slot(a, slot, Xs);
   if (rc) return rc;
   return smaug::adj_bwd(a, nullptr, ubar_next, ubar, thbar, t, static_cast<cudaStream_t>(stream), Xs);
+}
+
+extern "C" int smaug_adj_backward_tape_range(smaug_adj_t h, int32_t slot_lo, int32_t nsteps,
+                                             const double* gsteps, double* ubar, double* thbar,
+                                             double t0, int32_t n_lo, void* stream) {
+  smaug::clear_error();
+  if (!h || !ubar || !thbar || nsteps < 0) return smaug::set_error(SMAUG_E_INVALID, "bad argument");
+  Adjoint* a = HA(h);
+  if (slot_lo < 0 || slot_lo + nsteps > a->nslots)
+    return smaug::set_error(SMAUG_E_INVALID, "tape slots [%d, %d) outside [0, %d)", slot_lo, slot_lo + nsteps,
+                            a->nslots);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const long n6 = 6 * a->nc;
+  if (!a->ubar2) CUDA_TRY(cudaMalloc(&a->ubar2, sizeof(double) * n6));
+  double* cur = ubar;
+  for (int k = nsteps - 1; k >= 0; k--) {
+    if (gsteps) smaug::add_inplace<<<(unsigned)((n6 + 255) / 256), 256, 0, st>>>(cur, gsteps + k * n6, n6);
+    double* Xs[4];
+    int rc = smaug::tape_slot(a, slot_lo + k, Xs);
+    if (rc) return rc;
+    double* next = (cur == ubar) ? a->ubar2 : ubar;
+    // the time of absolute step n_lo + k, formed as the caller forms it
+    const double t = t0 + (double)(n_lo + k) * a->P.dt;
+    rc = smaug::adj_bwd(a, nullptr, cur, next, thbar, t, st, Xs, true);
+    if (rc) return rc;
+    cur = next;
+  }
+  if (cur != ubar) CUDA_TRY(cudaMemcpyAsync(ubar, cur, sizeof(double) * n6, cudaMemcpyDeviceToDevice, st));
+  return SMAUG_OK;
 }
 
 extern "C" int smaug_adj_backward(smaug_adj_t h, const double* u, const double* ubar_next, double* ubar,

@@ -26,6 +26,7 @@ EXPORTS = [
     "smaug_adj_create", "smaug_adj_set_driver", "smaug_adj_forward", "smaug_adj_backward",
     "smaug_adj_tape_reserve", "smaug_adj_forward_tape", "smaug_adj_backward_tape",
     "smaug_adj_destroy", "smaug_write_out_async", "smaug_wait_writes",
+    "smaug_adj_backward_tape_range",
 ]
 
 ERRORS = {1: "invalid", 2: "cuda", 3: "nomem", 4: "io", 5: "format", 6: "unsupported",
@@ -96,6 +97,8 @@ def lib():
         L.smaug_adj_tape_reserve.argtypes = [vp, ctypes.c_int32]
         L.smaug_adj_forward_tape.argtypes = [vp, vp, vp, ctypes.c_double, ctypes.c_int32, vp]
         L.smaug_adj_backward_tape.argtypes = [vp, ctypes.c_int32, vp, vp, vp, ctypes.c_double, vp]
+        L.smaug_adj_backward_tape_range.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, vp, vp, vp,
+                                                    ctypes.c_double, ctypes.c_int32, vp]
         L.smaug_adj_destroy.argtypes = [vp]
         _lib = L
     return _lib
