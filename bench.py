@@ -473,6 +473,72 @@ def _adjoint_case(args, sa, q, p, u0, pos, rhob, theta0, shift, obs_z, nsteps, r
     return line
 
 
+def accuracy_main(args):
+    """--workload accuracy: the mixed precision form against FP64 at the
+    configured run lengths -- 2D Orszag-Tang (1e-3 rho noise) 1024^2 and
+    4096^2 for 500 RK4 steps, the 3D stratified tube 256^3 for 1000 RK4
+    steps: relative L2 distance per evolved field, and both forms' rates
+    (CUDA events over the whole run).  Beside it, the sensitivity of the FP64
+    solution itself: an FP64 run whose evolved state is rounded to float once,
+    after step 10 (one rounding of the kind a float-storage form makes at
+    every stage), against the plain FP64 run."""
+    import numpy as np
+    import torch
+    from smaug_b200 import engine
+    cases = [("ot", 1024, 500), ("ot", 4096, 500), ("tube", 256, 1000)]
+    out = []
+    for kind, n, nsteps in cases:
+        states, ms = [], []
+        for prec, rounded in ((0, False), (1, False), (0, True)):
+            p, w, pos = (make_tube if kind == "tube" else make_case)(n, 1, prec)
+            nevo = p.nvar - (4 if p.ndim == 2 else 5)
+            e = engine.Engine(p, w, pos)
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            a.record()
+            if rounded:
+                e.step(10)
+                st = e.state()
+                st[:nevo] = st[:nevo].astype(np.float32).astype(np.float64)
+                e.set_state(st)
+                del st
+                e.step(nsteps - 10)
+            else:
+                e.step(nsteps)
+            b.record()
+            torch.cuda.synchronize()
+            ms.append(a.elapsed_time(b))
+            states.append(e.state()[:nevo])
+            e.close()
+            del w, pos
+
+        def rel(x):
+            r = []
+            for f in range(states[0].shape[0]):
+                d = float(np.sqrt(np.sum((x[f] - states[0][f]) ** 2)))
+                nrm = float(np.sqrt(np.sum(states[0][f] ** 2)))
+                r.append(d / nrm if nrm > 0 else d)
+            return r
+        errs, sens = rel(states[1]), rel(states[2])
+        cells = n ** (3 if kind == "tube" else 2)
+        dims = "x".join([str(n)] * (3 if kind == "tube" else 2))
+        out.append({"case": "%s %s, %d RK4 steps" % ("3D stratified tube" if kind == "tube" else
+                                                     "2D Orszag-Tang", dims, nsteps),
+                    "rel_l2_per_field": errs, "max": max(errs),
+                    "fp64_rounded_once_at_step_10_rel_l2_per_field": sens,
+                    "fp64_mcell_updates_per_s": cells * nsteps / (ms[0] / 1e3) / 1e6,
+                    "mixed_mcell_updates_per_s": cells * nsteps / (ms[1] / 1e3) / 1e6})
+        states = None
+    line = {"metric": "mixed vs FP64 relative L2 per evolved field at the configured run length",
+            "value": max(c["max"] for c in out[:2]), "unit": "relative L2 (2D cases)", "n_gpus": 1,
+            "steps": None, "warmup": 0, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64 vs f32 storage", "data": "synthetic", "target": 1e-5,
+            "config": {"workload": "Orszag-Tang 1024^2 and 4096^2 (500 steps), stratified tube 256^3 "
+                                   "(1000 steps), seeded"}, "cases": out}
+    print(json.dumps(line), flush=True)
+
+
 def snapshots_main(args):
     """--workload snapshots: RK4 steps of a 1024^2 Orszag-Tang grid with a
     reference .out snapshot every 10 steps (the driver's cfgsavefrequency
@@ -637,7 +703,8 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="ot", choices=["ot", "tube", "ensemble", "adjoint", "snapshots"])
+    ap.add_argument("--workload", default="ot", choices=["ot", "tube", "ensemble", "adjoint", "snapshots",
+                                                        "accuracy"])
     ap.add_argument("--adj-steps", type=int, default=400)
     ap.add_argument("--obs-z", type=float, default=3.0e6,
                     help="height of the observed v_z row for --workload adjoint [m]")
@@ -670,6 +737,9 @@ def main():
         return
     if args.workload == "snapshots" and args.impl != "reference":
         snapshots_main(args)
+        return
+    if args.workload == "accuracy" and args.impl != "reference":
+        accuracy_main(args)
         return
     if args.impl == "reference":
         reference_arm(args, ws, rank)
