@@ -242,18 +242,18 @@ def make_ensemble(nruns=64, seed=5, precision=1):
 
 def ensemble_main(args):
     """--workload ensemble: 64 uneven runs in one batch (one launch per stage
-    for all runs, 6-step CUDA graph cycles, autotuned launch shape) against
+    for all runs, 6-step CUDA graph cycles, autotuned tile and launch shape) against
     the same runs stepped one by one through their own engines."""
     import torch
     from smaug_b200 import engine
     prec = 0 if args.precision == "fp64" else 1
     runs = make_ensemble(args.nruns, precision=prec)
     cells = sum(r[3] for r in runs)
-    warm = max(args.warmup, 4)
+    warm = max(args.warmup, 8)
     b = engine.Batch([r[0] for r in runs], [r[1] for r in runs], [r[2] for r in runs])
     stream = torch.cuda.Stream()
     b.set_stream(stream.cuda_stream)
-    b.step(warm)            # the first 4 steps time the launch-shape candidates
+    b.step(warm)            # the first 8 steps time the (tile shape, grid) candidates
     torch.cuda.synchronize()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
@@ -265,6 +265,7 @@ def ensemble_main(args):
     b.sync()
     ms = ev0.elapsed_time(ev1)
     shape = b.launch_shape()
+    shape["tile"] = b.tile_shape()
     b.close()
     # one by one: each run alone, its own engine and stream, same step counts
     ms_single = 0.0

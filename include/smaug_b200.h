@@ -218,8 +218,16 @@ int smaug_batch_set_stream(smaug_batch_t b, void* stream);
 /* state / time of run `run`, as smaug_get_state / smaug_get_time */
 int smaug_batch_get_state(smaug_batch_t b, int32_t run, double* w);
 int smaug_batch_get_time(smaug_batch_t b, int32_t run, int64_t* it, double* t, double* dt);
-/* chosen grid (0 before tuning), the 4 candidate grids and their step times in ms */
+/* chosen grid (0 before tuning), the 4 candidate grids of the chosen tile
+   shape and their step times in ms */
 int smaug_batch_launch_shape(smaug_batch_t b, int32_t* grid, int32_t* candidates, float* ms);
+/* The batch's first steps time every (tile shape, grid) candidate and keep the
+   fastest: tile shapes 32x8 and 16x16, 4 grids each.  Chosen tile (0x0 before
+   tuning) and the 8 step times in ms (32x8's four grids, then 16x16's; 0 for
+   a candidate not timed). */
+int smaug_batch_tile_shape(smaug_batch_t b, int32_t* tx, int32_t* ty, float* ms);
+/* Use only tile shape tx x ty (32x8 or 16x16); call before the first step. */
+int smaug_batch_pin_tile_shape(smaug_batch_t b, int32_t tx, int32_t ty);
 int smaug_batch_destroy(smaug_batch_t b);
 
 /* ---- adjoint of one RK4 step (2D, FP64, dt held fixed) -------------------

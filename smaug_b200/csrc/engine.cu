@@ -910,18 +910,33 @@ namespace smaug {
 
 constexpr int BATCH_CYCLE = 6;
 
+// tile shapes of the batched kernel, each its own instantiation
+struct BatchShape {
+  int tx, ty;
+  cudaError_t (*launch)(int, bool, const KParams*, const KBufs*, const int4*, int, int, cudaStream_t);
+  cudaError_t (*set_attributes)();
+  int (*max_blocks_per_sm)(bool);
+};
+constexpr int NSHAPES = 2;
+static const BatchShape kShapes[NSHAPES] = {
+    {32, 8, t32x8::launch_batch2d, t32x8::batch2d_set_attributes, t32x8::batch2d_max_blocks_per_sm},
+    {16, 16, t16x16::launch_batch2d, t16x16::batch2d_set_attributes, t16x16::batch2d_max_blocks_per_sm},
+};
+
 struct Batch {
   std::vector<Engine*> runs;
   bool mix = false;
   cudaStream_t stream = nullptr;
   KParams* d_K = nullptr;   // [nruns]
   KBufs* d_B = nullptr;     // [4 stages][2 parities][3 ring slots][nruns]
-  int4* d_tiles = nullptr;  // (run, tile x, tile y)
-  int ntiles = 0;
+  int4* d_tiles[NSHAPES] = {nullptr, nullptr};  // (run, tile x, tile y) per tile shape
+  int ntiles[NSHAPES] = {0, 0};
+  int shape = 0;            // tile shape in use (index into kShapes)
+  int pinned = -1;          // tile shape fixed by the caller (-1: tuned)
   int grid = 0;             // persistent blocks per launch (0: not chosen yet)
-  int grid_candidates[4] = {0, 0, 0, 0};
-  float grid_ms[4] = {0, 0, 0, 0};
-  int tuned = 0;            // candidates timed so far
+  int grid_candidates[NSHAPES][4] = {};
+  float grid_ms[NSHAPES][4] = {};
+  int tuned = 0;            // (shape, grid) candidates timed so far
   long steps = 0;
   cudaGraphExec_t cycle = nullptr;
   cudaStream_t own_stream = nullptr;  // the batch's stream while a caller stream is set
@@ -933,7 +948,7 @@ static void free_batch(Batch* b) {
   if (b->cycle) cudaGraphExecDestroy(b->cycle);
   cudaFree(b->d_K);
   cudaFree(b->d_B);
-  cudaFree(b->d_tiles);
+  for (int s = 0; s < NSHAPES; s++) cudaFree(b->d_tiles[s]);
   for (Engine* e : b->runs) free_engine(e);
   cudaStreamDestroy(b->own_stream ? b->own_stream : b->stream);
   delete b;
@@ -941,14 +956,16 @@ static void free_batch(Batch* b) {
 
 static int batch_variant(int stage, int parity, int ring) { return (stage * 2 + parity) * 3 + ring; }
 
-// one RK4 step of every run, starting at global step index k of the batch
-static int batch_enqueue_step(Batch* b, long k, int grid) {
+// one RK4 step of every run, starting at global step index k of the batch,
+// with tile shape `shape` and `grid` persistent blocks
+static int batch_enqueue_step(Batch* b, long k, int shape, int grid) {
   const int nr = (int)b->runs.size();
   const int parity = (int)(k % 2);
   for (int s = 0; s < 4; s++) {
     const int ring = (int)((4 * k + s) % 3);
-    CUDA_TRY(launch_batch2d(SMAUG_INT_RK4, b->mix, b->d_K, b->d_B + (size_t)batch_variant(s, parity, ring) * nr,
-                            b->d_tiles, b->ntiles, grid, b->stream));
+    CUDA_TRY(kShapes[shape].launch(SMAUG_INT_RK4, b->mix, b->d_K,
+                                   b->d_B + (size_t)batch_variant(s, parity, ring) * nr, b->d_tiles[shape],
+                                   b->ntiles[shape], grid, b->stream));
   }
   return SMAUG_OK;
 }
@@ -994,7 +1011,7 @@ static int batch_create(int nruns, const smaug_params_t* const* params, const do
   // parameter blocks, the 24 buffer-block variants of every run, the tile list
   std::vector<KParams> K(nruns);
   std::vector<KBufs> B((size_t)24 * nruns);
-  std::vector<int4> tiles;
+  std::vector<int4> tiles[NSHAPES];
   for (int r = 0; r < nruns; r++) {
     Engine* e = b->runs[r];
     K[r] = e->K;
@@ -1003,11 +1020,13 @@ static int batch_create(int nruns, const smaug_params_t* const* params, const do
       for (int par = 0; par < 2; par++)
         for (int ring = 0; ring < 3; ring++)
           B[(size_t)batch_variant(s, par, ring) * nruns + r] = rk4_kbufs(e, s, par, ring);
-    const int tx = (e->K.n0 - 4 + TX - 1) / TX, ty = (e->K.n1 - 4 + TY - 1) / TY;
-    for (int j = 0; j < ty; j++)
-      for (int i = 0; i < tx; i++) tiles.push_back(make_int4(r, i, j, 0));
+    for (int sh = 0; sh < NSHAPES; sh++) {
+      const int sx = kShapes[sh].tx, sy = kShapes[sh].ty;
+      const int tx = (e->K.n0 - 4 + sx - 1) / sx, ty = (e->K.n1 - 4 + sy - 1) / sy;
+      for (int j = 0; j < ty; j++)
+        for (int i = 0; i < tx; i++) tiles[sh].push_back(make_int4(r, i, j, 0));
+    }
   }
-  b->ntiles = (int)tiles.size();
 #define B_TRY(call)                                                                             \
   do {                                                                                          \
     cudaError_t _e = (call);                                                                    \
@@ -1017,50 +1036,63 @@ static int batch_create(int nruns, const smaug_params_t* const* params, const do
   } while (0)
   B_TRY(cudaMalloc(&b->d_K, sizeof(KParams) * nruns));
   B_TRY(cudaMalloc(&b->d_B, sizeof(KBufs) * B.size()));
-  B_TRY(cudaMalloc(&b->d_tiles, sizeof(int4) * tiles.size()));
   B_TRY(cudaMemcpy(b->d_K, K.data(), sizeof(KParams) * nruns, cudaMemcpyHostToDevice));
   B_TRY(cudaMemcpy(b->d_B, B.data(), sizeof(KBufs) * B.size(), cudaMemcpyHostToDevice));
-  B_TRY(cudaMemcpy(b->d_tiles, tiles.data(), sizeof(int4) * tiles.size(), cudaMemcpyHostToDevice));
-  B_TRY(batch2d_set_attributes());
-  // launch-shape candidates: 1, 2 or the occupancy limit of blocks per SM
-  // (persistent), or one block per tile
   int dev = 0, nsm = 0;
   B_TRY(cudaGetDevice(&dev));
   B_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-  int occ = batch2d_max_blocks_per_sm(b->mix);
-  if (occ < 1) occ = 1;
-  b->grid_candidates[0] = nsm;
-  b->grid_candidates[1] = 2 * nsm < b->ntiles ? 2 * nsm : b->ntiles;
-  b->grid_candidates[2] = occ * nsm < b->ntiles ? occ * nsm : b->ntiles;
-  b->grid_candidates[3] = b->ntiles;
+  for (int sh = 0; sh < NSHAPES; sh++) {
+    const int nt = (int)tiles[sh].size();
+    b->ntiles[sh] = nt;
+    B_TRY(cudaMalloc(&b->d_tiles[sh], sizeof(int4) * nt));
+    B_TRY(cudaMemcpy(b->d_tiles[sh], tiles[sh].data(), sizeof(int4) * nt, cudaMemcpyHostToDevice));
+    B_TRY(kShapes[sh].set_attributes());
+    // launch-shape candidates: 1, 2 or the occupancy limit of blocks per SM
+    // (persistent), or one block per tile
+    int occ = kShapes[sh].max_blocks_per_sm(b->mix);
+    if (occ < 1) occ = 1;
+    int* gc = b->grid_candidates[sh];
+    gc[0] = nsm < nt ? nsm : nt;
+    gc[1] = 2 * nsm < nt ? 2 * nsm : nt;
+    gc[2] = occ * nsm < nt ? occ * nsm : nt;
+    gc[3] = nt;
+  }
 #undef B_TRY
   *out = b;
   return SMAUG_OK;
 }
 
-// Launch-shape autotuning: the first four steps run with the four candidate
-// grids, each timed with events; the fastest is kept.  The grid only changes
-// which block processes which tile, so results do not depend on it.
+// Tile- and launch-shape autotuning: the first steps run with every
+// (tile shape, grid) candidate -- 2 tile shapes x 4 grids, or the 4 grids of
+// a pinned shape -- each timed with events; the fastest is kept.  Neither
+// choice changes a cell's arithmetic (the tile only decides which block
+// stages and computes it), so results do not depend on them.
 static int batch_tune(Batch* b, int* nsteps) {
   cudaEvent_t ev[2];
   CUDA_TRY(cudaEventCreate(&ev[0]));
   CUDA_TRY(cudaEventCreate(&ev[1]));
-  for (int c = b->tuned; c < 4 && *nsteps > 0; c++) {
+  for (int c = b->tuned; c < NSHAPES * 4 && *nsteps > 0; c++) {
+    const int sh = c / 4, g = c % 4;
+    b->tuned = c + 1;
+    if (b->pinned >= 0 && sh != b->pinned) continue;
     CUDA_TRY(cudaEventRecord(ev[0], b->stream));
-    int rc = batch_enqueue_step(b, b->steps, b->grid_candidates[c]);
+    int rc = batch_enqueue_step(b, b->steps, sh, b->grid_candidates[sh][g]);
     if (rc) return rc;
     CUDA_TRY(cudaEventRecord(ev[1], b->stream));
     CUDA_TRY(cudaEventSynchronize(ev[1]));
-    CUDA_TRY(cudaEventElapsedTime(&b->grid_ms[c], ev[0], ev[1]));
+    CUDA_TRY(cudaEventElapsedTime(&b->grid_ms[sh][g], ev[0], ev[1]));
     batch_advance_bookkeeping(b, 1);
     (*nsteps)--;
-    b->tuned = c + 1;
   }
-  if (b->tuned == 4) {
-    int best = 0;
-    for (int c = 1; c < 4; c++)
-      if (b->grid_ms[c] < b->grid_ms[best]) best = c;
-    b->grid = b->grid_candidates[best];
+  if (b->tuned == NSHAPES * 4) {
+    int bs = -1, bg = 0;
+    for (int sh = 0; sh < NSHAPES; sh++) {
+      if (b->pinned >= 0 && sh != b->pinned) continue;
+      for (int g = 0; g < 4; g++)
+        if (bs < 0 || b->grid_ms[sh][g] < b->grid_ms[bs][bg]) bs = sh, bg = g;
+    }
+    b->shape = bs;
+    b->grid = b->grid_candidates[bs][bg];
   }
   cudaEventDestroy(ev[0]);
   cudaEventDestroy(ev[1]);
@@ -1078,7 +1110,7 @@ static int batch_enqueue(Batch* b, int nsteps) {
         cudaGraph_t g = nullptr;
         CUDA_TRY(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
         int rc = SMAUG_OK;
-        for (int k = 0; k < BATCH_CYCLE && !rc; k++) rc = batch_enqueue_step(b, k, b->grid);
+        for (int k = 0; k < BATCH_CYCLE && !rc; k++) rc = batch_enqueue_step(b, k, b->shape, b->grid);
         cudaError_t ce = cudaStreamEndCapture(b->stream, &g);
         if (rc) return rc;
         if (ce != cudaSuccess) return set_error(SMAUG_E_CUDA, "graph capture: %s", cudaGetErrorString(ce));
@@ -1090,7 +1122,7 @@ static int batch_enqueue(Batch* b, int nsteps) {
       batch_advance_bookkeeping(b, BATCH_CYCLE);
       nsteps -= BATCH_CYCLE;
     } else {
-      int rc = batch_enqueue_step(b, b->steps, b->grid);
+      int rc = batch_enqueue_step(b, b->steps, b->shape, b->grid);
       if (rc) return rc;
       batch_advance_bookkeeping(b, 1);
       nsteps--;
@@ -1181,10 +1213,38 @@ extern "C" int smaug_batch_launch_shape(smaug_batch_t h, int32_t* grid, int32_t*
   Batch* b = HB(h);
   if (grid) *grid = b->grid;
   for (int c = 0; c < 4; c++) {
-    if (candidates) candidates[c] = b->grid_candidates[c];
-    if (ms) ms[c] = b->grid_ms[c];
+    if (candidates) candidates[c] = b->grid_candidates[b->shape][c];
+    if (ms) ms[c] = b->grid_ms[b->shape][c];
   }
   return SMAUG_OK;
+}
+
+extern "C" int smaug_batch_tile_shape(smaug_batch_t h, int32_t* tx, int32_t* ty, float* ms) {
+  smaug::clear_error();
+  if (!h) return smaug::set_error(SMAUG_E_INVALID, "null handle");
+  Batch* b = HB(h);
+  const bool chosen = b->grid != 0;
+  if (tx) *tx = chosen ? smaug::kShapes[b->shape].tx : 0;
+  if (ty) *ty = chosen ? smaug::kShapes[b->shape].ty : 0;
+  if (ms)
+    for (int sh = 0; sh < smaug::NSHAPES; sh++)
+      for (int g = 0; g < 4; g++) ms[sh * 4 + g] = b->grid_ms[sh][g];
+  return SMAUG_OK;
+}
+
+extern "C" int smaug_batch_pin_tile_shape(smaug_batch_t h, int32_t tx, int32_t ty) {
+  smaug::clear_error();
+  if (!h) return smaug::set_error(SMAUG_E_INVALID, "null handle");
+  Batch* b = HB(h);
+  if (b->tuned > 0 || b->grid != 0)
+    return smaug::set_error(SMAUG_E_INVALID, "the tile shape is chosen at the first step: pin it before");
+  for (int sh = 0; sh < smaug::NSHAPES; sh++)
+    if (smaug::kShapes[sh].tx == tx && smaug::kShapes[sh].ty == ty) {
+      b->pinned = sh;
+      b->shape = sh;
+      return SMAUG_OK;
+    }
+  return smaug::set_error(SMAUG_E_INVALID, "tile shape %dx%d not built (32x8, 16x16)", tx, ty);
 }
 
 extern "C" int smaug_batch_destroy(smaug_batch_t h) {

@@ -301,11 +301,17 @@ cudaError_t launch_stage3d_any(int mode, bool mix, const KParams& K, const KBufs
 cudaError_t stage2d_set_attributes();
 cudaError_t stage3d_set_attributes();
 
-// batched 2D stages (batch.cu): Ks/Bs per run in device memory, tiles =
-// (run, tile x, tile y) work list, `grid` persistent blocks
-cudaError_t launch_batch2d(int mode, bool mix, const KParams* Ks, const KBufs* Bs, const int4* tiles,
-                           int ntiles, int grid, cudaStream_t st);
-cudaError_t batch2d_set_attributes();
-int batch2d_max_blocks_per_sm(bool mix);
+// batched 2D stages (batch_kernel.cuh), one instantiation per tile shape
+// (batch.cu: 32x8, batch16.cu: 16x16): Ks/Bs per run in device memory,
+// tiles = (run, tile x, tile y) work list of that shape, `grid` persistent
+// blocks
+#define SMAUG_BATCH_DECL                                                                        \
+  cudaError_t launch_batch2d(int mode, bool mix, const KParams* Ks, const KBufs* Bs,           \
+                             const int4* tiles, int ntiles, int grid, cudaStream_t st);         \
+  cudaError_t batch2d_set_attributes();                                                         \
+  int batch2d_max_blocks_per_sm(bool mix);
+namespace t32x8 { SMAUG_BATCH_DECL }
+namespace t16x16 { SMAUG_BATCH_DECL }
+#undef SMAUG_BATCH_DECL
 
 }  // namespace smaug

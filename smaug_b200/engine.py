@@ -26,7 +26,7 @@ EXPORTS = [
     "smaug_adj_create", "smaug_adj_set_driver", "smaug_adj_forward", "smaug_adj_backward",
     "smaug_adj_tape_reserve", "smaug_adj_forward_tape", "smaug_adj_backward_tape",
     "smaug_adj_destroy", "smaug_write_out_async", "smaug_wait_writes",
-    "smaug_adj_backward_tape_range",
+    "smaug_adj_backward_tape_range", "smaug_batch_tile_shape", "smaug_batch_pin_tile_shape",
 ]
 
 ERRORS = {1: "invalid", 2: "cuda", 3: "nomem", 4: "io", 5: "format", 6: "unsupported",
@@ -86,6 +86,9 @@ def lib():
         L.smaug_batch_set_stream.argtypes = [vp, vp]
         L.smaug_batch_get_state.argtypes = [vp, ctypes.c_int32, dp]
         L.smaug_batch_get_time.argtypes = [vp, ctypes.c_int32, ctypes.POINTER(ctypes.c_int64), dp, dp]
+        L.smaug_batch_tile_shape.argtypes = [vp, ctypes.POINTER(ctypes.c_int32),
+                                             ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_float)]
+        L.smaug_batch_pin_tile_shape.argtypes = [vp, ctypes.c_int32, ctypes.c_int32]
         L.smaug_batch_launch_shape.argtypes = [vp, ctypes.POINTER(ctypes.c_int32),
                                                ctypes.POINTER(ctypes.c_int32),
                                                ctypes.POINTER(ctypes.c_float)]
@@ -303,6 +306,20 @@ class Batch:
         ms = (ctypes.c_float * 4)()
         _check(lib().smaug_batch_launch_shape(self.h, ctypes.byref(g), cand, ms))
         return {"grid": int(g.value), "candidates": list(cand), "ms": [float(v) for v in ms]}
+
+    def tile_shape(self):
+        """The tile shape the autotuner chose ((0, 0) before the first steps)
+        and the step time of every (tile shape, grid) candidate."""
+        tx, ty = ctypes.c_int32(0), ctypes.c_int32(0)
+        ms = (ctypes.c_float * 8)()
+        _check(lib().smaug_batch_tile_shape(self.h, ctypes.byref(tx), ctypes.byref(ty), ms))
+        return {"tile": (int(tx.value), int(ty.value)),
+                "ms": {"32x8": [float(v) for v in ms[:4]], "16x16": [float(v) for v in ms[4:]]}}
+
+    def pin_tile_shape(self, tx, ty):
+        """Use only the tile shape tx x ty (32x8 or 16x16); before the first step."""
+        _check(lib().smaug_batch_pin_tile_shape(self.h, int(tx), int(ty)))
+        return self
 
     def close(self):
         if getattr(self, "h", None):

@@ -43,16 +43,29 @@ def ensemble(precision):
     return runs
 
 
+@pytest.mark.parametrize("pin", [None, (32, 8), (16, 16)])
 @pytest.mark.parametrize("precision,tol", [(P.PREC_FP64, 1e-12), (P.PREC_MIXED, 1e-6)])
-def test_batch_matches_single_runs(engine_lib, precision, tol):
+def test_batch_matches_single_runs(engine_lib, precision, tol, pin):
+    """Every run of a batch against the same run stepped alone, with the tile
+    shape chosen by the autotuner or pinned to each built shape (the
+    single-run kernel uses 32x8 tiles)."""
     runs = ensemble(precision)
     b = engine_lib.Batch([r[0] for r in runs], [r[1] for r in runs], [r[2] for r in runs])
-    b.step(13)  # 4 tuning steps, one 6-step graph cycle, 3 single steps
+    if pin:
+        b.pin_tile_shape(*pin)
+    nfirst = 20  # 8 (4 pinned) tuning steps, single steps, a 6-step graph cycle from step 12
+    b.step(nfirst)
     shape = b.launch_shape()
     assert shape["grid"] in shape["candidates"]
+    tile = b.tile_shape()
+    assert tile["tile"] in ((32, 8), (16, 16))
+    if pin:
+        assert tile["tile"] == pin
+    else:
+        assert all(v > 0 for v in tile["ms"]["32x8"] + tile["ms"]["16x16"])
     for i, (p, w, pos) in enumerate(runs):
         e = engine_lib.Engine(p, w, pos)
-        e.step(13)
+        e.step(nfirst)
         ref = e.state()
         it, t, dt = e.time()
         e.close()
@@ -61,12 +74,12 @@ def test_batch_matches_single_runs(engine_lib, precision, tol):
             assert rel_l2(got[f], ref[f]) <= tol, (i, f, rel_l2(got[f], ref[f]))
         assert np.array_equal(got[6:], ref[6:])
         bit, bt, bdt = b.time(i)
-        assert bit == it == 13
+        assert bit == it == nfirst
         assert abs(bt - t) <= 1e-12 * abs(t)
-    b.step(7)  # continues from a cycle boundary that is not 0 mod 6
+    b.step(7)  # continues from a step that is not 0 mod 6
     for i, (p, w, pos) in enumerate(runs[:2]):
         e = engine_lib.Engine(p, w, pos)
-        e.step(20)
+        e.step(nfirst + 7)
         ref = e.state()
         e.close()
         got = b.state(i)
@@ -86,3 +99,19 @@ def test_batch_rejects(engine_lib):
     with pytest.raises(engine_lib.SmaugError) as e:
         engine_lib.Batch([p64, pmx], [w, w], [pos, pos])
     assert e.value.code == 6
+
+
+def test_batch_pin_tile_shape_rejects(engine_lib):
+    """Only built tile shapes can be pinned, and only before the first step."""
+    w, pos, dx = ot_rect(40, 40, seed=1)
+    p = params_for(w, dx, integrator=P.INT_RK4)
+    b = engine_lib.Batch([p], [w], [pos])
+    with pytest.raises(engine_lib.SmaugError) as e:
+        b.pin_tile_shape(8, 8)
+    assert e.value.code == 1
+    assert b.tile_shape()["tile"] == (0, 0)
+    b.step(1)
+    with pytest.raises(engine_lib.SmaugError) as e:
+        b.pin_tile_shape(16, 16)
+    assert e.value.code == 1
+    b.close()
