@@ -199,9 +199,10 @@ int smaug_destroy(smaug_handle_t h);
  * size, boundary types, background fields and driver advance together with
  * classical RK4: every stage of every run is one launch over the tile list of
  * all runs, and a cycle of 6 steps is captured once into a CUDA graph and
- * replayed.  All runs share one precision form.  The first 4 steps time 4
- * launch shapes (1 and 2 blocks per SM, the occupancy limit per SM, one block
- * per tile) and keep the fastest; results do not depend on the shape.  Each
+ * replayed.  All runs share one precision form.  The first 8 steps time 2
+ * tile shapes (32x8, 16x16) x 4 launch shapes (1 and 2 blocks per SM, the
+ * occupancy limit per SM, one block per tile) and keep the fastest; results
+ * do not depend on either shape.  Each
  * run's results equal those of the same run stepped alone with smaug_step. */
 typedef struct smaug_batch_s* smaug_batch_t;
 

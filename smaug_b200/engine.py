@@ -250,7 +250,8 @@ class Engine:
 
 class Batch:
     """An ensemble of independent 2D runs advanced together (RK4): one launch
-    per stage for all runs, a 6-step cycle replayed from a CUDA graph."""
+    per stage for all runs, a 6-step cycle replayed from a CUDA graph; the
+    first 8 steps choose the tile and launch shape by timing."""
 
     def __init__(self, params_list, w_list, pos_list):
         n = len(params_list)
