@@ -281,10 +281,12 @@ const char* smaug_version(void);
 
 /*
  * One reference (Euler) step that allocates nothing.  No counterpart in the
- * reference: it exists for callers that cannot call cudaMalloc -- code
- * recording a CUDA graph by stream capture, hosts that own all device memory
- * through their own pool or budget, loops that must not take the implicit
- * synchronisation of an allocation.
+ * reference.  It is for callers that cannot call cudaMalloc: applications
+ * that reserve their device memory up front (a caching pool, a fixed budget
+ * on a shared GPU) and cannot satisfy or do not allow allocations made behind
+ * their back, plugins whose host forbids allocation inside its step callback,
+ * and loops running beside other streams that cudaFree's implicit device-wide
+ * synchronisation would stall.
  *   w_in, w_out : DEVICE buffers, NVAR*ncells doubles each, reference layout;
  *                 w_in needs valid ghost layers (as left by a previous step);
  *                 w_out receives the whole state (backgrounds copied).
@@ -295,10 +297,12 @@ const char* smaug_version(void);
  * 2D only, no driver term, at most 8192 cells per dimension (ghosts
  * included); larger grids are rejected with SMAUG_E_UNSUPPORTED.  Scratch
  * lives in one static device array of 196,864 bytes per GPU, kept until the
- * process exits and shared by every call: calls whose GPU work overlaps (other
- * threads or streams) race on it and must be serialised by the caller.  The
- * first call on a device looks up that array's device address; make that
- * first call before any stream capture.  Returns after the step completed.
+ * process exits and shared by every call, which clears the parts that must
+ * start at zero: calls whose GPU work overlaps (other threads or streams)
+ * race on it and must be serialised by the caller.  The first call on a
+ * device looks up that array's device address and keeps it for the rest of
+ * the process (so it does not survive a cudaDeviceReset); make that first
+ * call before any stream capture.  Returns after the step completed.
  */
 int smaug_euler_step_noalloc(const smaug_params_t* p, const double* w_in, double* w_out,
                              const double* delx, double* dt, void* stream);

@@ -33,7 +33,8 @@ import sys
 import tempfile
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REFROOT = "/root/reference/smaug"
+# the reference checkout (its smaug/ project directory); SMAUG_REFERENCE overrides
+REFROOT = os.environ.get("SMAUG_REFERENCE", "/root/reference/smaug")
 OUT = os.path.join(HERE, "_ref")
 
 # sed instantiation table of src/Makefile:163-227: object -> [(template, id)]

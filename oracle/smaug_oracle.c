@@ -25,7 +25,7 @@
  * explicitly by params->pad_model.
  *
  * Parity status: pinned against the reference binary built from the
- * reference's own sources (oracle/build_ref.sh) and run on a B200; see the
+ * reference's own sources (oracle/build_ref.py) and run on a B200; see the
  * golden fixtures under tests/golden/.
  */
 #include <math.h>

@@ -1067,8 +1067,18 @@ static int batch_create(int nruns, const smaug_params_t* const* params, const do
 // a pinned shape -- each timed with events; the fastest is kept.  Neither
 // choice changes a cell's arithmetic (the tile only decides which block
 // stages and computes it), so results do not depend on them.
+// the two timing events of batch_tune, destroyed on every exit path
+struct EventPair {
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  ~EventPair() {
+    for (cudaEvent_t& e : ev)
+      if (e) cudaEventDestroy(e);
+  }
+};
+
 static int batch_tune(Batch* b, int* nsteps) {
-  cudaEvent_t ev[2];
+  EventPair pair;
+  cudaEvent_t* ev = pair.ev;
   CUDA_TRY(cudaEventCreate(&ev[0]));
   CUDA_TRY(cudaEventCreate(&ev[1]));
   for (int c = b->tuned; c < NSHAPES * 4 && *nsteps > 0; c++) {
@@ -1094,8 +1104,6 @@ static int batch_tune(Batch* b, int* nsteps) {
     b->shape = bs;
     b->grid = b->grid_candidates[bs][bg];
   }
-  cudaEventDestroy(ev[0]);
-  cudaEventDestroy(ev[1]);
   return SMAUG_OK;
 }
 
@@ -1112,8 +1120,11 @@ static int batch_enqueue(Batch* b, int nsteps) {
         int rc = SMAUG_OK;
         for (int k = 0; k < BATCH_CYCLE && !rc; k++) rc = batch_enqueue_step(b, k, b->shape, b->grid);
         cudaError_t ce = cudaStreamEndCapture(b->stream, &g);
-        if (rc) return rc;
-        if (ce != cudaSuccess) return set_error(SMAUG_E_CUDA, "graph capture: %s", cudaGetErrorString(ce));
+        if (rc || ce != cudaSuccess) {
+          if (g) cudaGraphDestroy(g);
+          if (rc) return rc;
+          return set_error(SMAUG_E_CUDA, "graph capture: %s", cudaGetErrorString(ce));
+        }
         ce = cudaGraphInstantiate(&b->cycle, g, 0);
         cudaGraphDestroy(g);
         if (ce != cudaSuccess) return set_error(SMAUG_E_CUDA, "graph instantiate: %s", cudaGetErrorString(ce));
@@ -1257,15 +1268,16 @@ extern "C" int smaug_batch_destroy(smaug_batch_t h) {
 // ===========================================================================
 // Allocation-free Euler step
 // ===========================================================================
-// Some callers cannot call cudaMalloc: code that records its work into a
-// CUDA graph by stream capture (allocation is not allowed while a capture is
-// active), hosts that hand the library memory they already own from their
-// own pool or a fixed device budget, and latency-critical loops where an
-// allocation's implicit device synchronisation would stall other streams.
-// smaug_euler_step_noalloc serves them: the caller passes device buffers for
-// the input and output state, and every piece of scratch the step needs (CFL
-// maxima, dt and time words, the error flag, the 1D metric and the stray-pad
-// source table) lives in the file-scope array below.
+// Some callers cannot call cudaMalloc: applications that reserve their device
+// memory up front (a framework's caching pool, a fixed per-process budget on
+// a shared GPU) and refuse or cannot satisfy allocations made behind their
+// back, plugins whose host forbids allocation inside its step callback, and
+// loops that run beside other streams, where cudaFree's implicit device-wide
+// synchronisation would stall them.  smaug_euler_step_noalloc serves them:
+// the caller passes device buffers for the input and output state, and every
+// piece of scratch the step needs (CFL maxima, dt and time words, the error
+// flag, the 1D metric and the stray-pad source table) lives in the
+// file-scope array below.
 namespace smaug {
 
 // Largest grid (cells per dimension, ghosts included) the array serves.
@@ -1282,7 +1294,8 @@ constexpr size_t NOALLOC_SCRATCH_BYTES = NA_PAD + 2 * NOALLOC_MAXN * sizeof(int)
 static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
 
 // Device address of g_noalloc_scratch per device (the host-side symbol is a
-// stand-in, not a device address); filled on a device's first call.
+// stand-in, not a device address); looked up once, on a device's first call,
+// and kept for the life of the process (a cudaDeviceReset invalidates it).
 constexpr int NA_MAXDEV = 64;
 static unsigned char* g_na_ptr[NA_MAXDEV] = {nullptr};
 static std::mutex g_na_mu;

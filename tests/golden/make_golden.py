@@ -5,8 +5,9 @@ these fixtures are produced by running the reference's own GPU binary (built
 from its sources by oracle/build_ref.py) on a B200, on inputs written here:
 
   python tests/golden/make_golden.py prepare   # here: .ini inputs + reference builds
-  python tests/golden/make_golden.py run       # on the GPU box: run the binaries
-  python tests/golden/make_golden.py collect   # here: .out files -> *.npz fixtures
+  python tests/golden/make_golden.py run --runs DIR      # on a GPU machine: run the binaries
+  python tests/golden/make_golden.py collect --runs DIR  # here: .out files -> *.npz fixtures
+(an optional comma-separated list of case names after the command selects cases)
 
 Cases (Orszag-Tang on [0,2pi]^2, seeded 1e-3 rho noise, the reference OT
 model parameters with PGAMMA 1.66666667, courant 0.3, DT 1, moddton on):
@@ -52,7 +53,11 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
 WORK = os.path.join(HERE, "_inputs")          # git-ignored; travels to the GPU box
-RUNS = os.path.join(ROOT, "gpurun_out", "gold")
+# directory holding the reference runs' .out files (one sub-directory per
+# case): `run` writes it on the GPU machine, `collect` reads it here after the
+# caller has copied it back.  `--runs DIR` or SMAUG_GOLDEN_RUNS selects it;
+# the default is git-ignored.
+RUNS = os.environ.get("SMAUG_GOLDEN_RUNS", os.path.join(HERE, "_runs"))
 
 # name: (nx, ny, seed, NT, steps kept[, boundary types per dim])
 CASES = {
@@ -139,8 +144,22 @@ def _build3(name, nx, ny, nz, nt, bt_ref=None, defines=()):
                                PGRAV2="0.0", **extra)
 
 
+def _parse_args(argv):
+    """command [case,case,...] [--runs DIR]"""
+    global RUNS
+    args = list(argv)
+    if "--runs" in args:
+        k = args.index("--runs")
+        RUNS = os.path.abspath(args[k + 1])
+        del args[k:k + 2]
+    return args
+
+
+ARGS = []
+
+
 def _selected(table):
-    want = sys.argv[2].split(",") if len(sys.argv) > 2 else None
+    want = ARGS[1].split(",") if len(ARGS) > 1 else None
     return {k: v for k, v in table.items() if want is None or k in want}
 
 
@@ -260,4 +279,5 @@ def collect():
 
 
 if __name__ == "__main__":
-    {"prepare": prepare, "run": run, "collect": collect}[sys.argv[1]]()
+    ARGS = _parse_args(sys.argv[1:])
+    {"prepare": prepare, "run": run, "collect": collect}[ARGS[0]]()

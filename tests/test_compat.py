@@ -20,7 +20,9 @@ from golden_util import load
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 HDR = os.path.join(ROOT, "include", "smaug_compat.h")
 PKG = os.path.join(ROOT, "smaug_b200")
-REFINC = "/root/reference/smaug/include"
+from oracle.build_ref import REFROOT  # noqa: E402  (SMAUG_REFERENCE overrides)
+
+REFINC = os.path.join(REFROOT, "include")
 MACROS = {"2d": "-DUSE_SAC", "3d": "-DUSE_SAC_3D"}
 
 

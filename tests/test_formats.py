@@ -11,7 +11,9 @@ import pytest
 from smaug_b200 import formats
 from tests.util import ot_rect, params_for
 
-REF_TILE = "/root/reference/smaug/configs/zero1_ot_asc_252_np0202_000.ini"
+from oracle.build_ref import REFROOT  # noqa: E402  (SMAUG_REFERENCE overrides)
+
+REF_TILE = os.path.join(REFROOT, "configs", "zero1_ot_asc_252_np0202_000.ini")
 
 
 def test_ini_roundtrip_c_reader(engine_lib, tmp_path):

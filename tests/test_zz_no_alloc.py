@@ -1,10 +1,10 @@
 """The allocation-free Euler step (smaug_euler_step_noalloc) against the
 engine's regular Euler step, through the C ABI.
 
-The entry point serves callers that cannot call cudaMalloc -- stream-captured
-CUDA graphs, hosts owning all device memory through their own pool, loops that
-must not take an allocation's device synchronisation -- so its scratch lives in
-one static device array.  The test owns the device buffers (torch), calls the
+The entry point serves callers that cannot call cudaMalloc -- applications that
+reserve their device memory up front, plugins whose host forbids allocating in
+its step callback, loops that cudaFree's device-wide synchronisation would
+stall -- so its scratch lives in one static device array.  The test owns the device buffers (torch), calls the
 entry point twice in a row (the second call reuses the array with the first
 call's leftovers), and checks both outputs against two regular steps:
 relative L2 per evolved field <= 1e-12, the same tolerance as the parity tests.
