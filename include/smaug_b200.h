@@ -79,6 +79,10 @@ extern "C" {
 /* user source (driver) kinds */
 #define SMAUG_DRIVER_NONE 0
 #define SMAUG_DRIVER_GAUSS 1  /* m_0 += dt * v(x,t) * rho_t, v Gaussian in space */
+/* the same term in one step only: the step whose counter (the reference's
+   p->it = n, src/iosmaug.c:498) equals drv_step -- the reference's spicule1
+   model kicks at p->it == 1 only (models/usersource.cu.spicule1:67-131) */
+#define SMAUG_DRIVER_GAUSS_STEP 2
 
 /*
  * Run parameters.  Mirrors the fields of the reference's struct params
@@ -100,7 +104,9 @@ typedef struct smaug_params {
   int32_t stencil_order;    /* flux-divergence derivative grad3dn: 4 (or 0) the
                                4th-order default, 6 the reference's USE_DORDER3
                                build (src/gradops.cu:450-453) */
-  int32_t reserved_i[6];
+  int32_t drv_step;         /* SMAUG_DRIVER_GAUSS_STEP: the step counter value at
+                               which the driver acts */
+  int32_t reserved_i[5];
   double dx[3];             /* p->dx: (xmax-xmin)/(n-4), used by the dt rule */
   double dt;                /* p->dt at start (the reference sets 1e-8 when moddton) */
   double dtmax;             /* DT: adaptive dt is accepted only below this */

@@ -78,9 +78,11 @@ def _set_define(text, name, value):
     return pat.sub("#define %s %s" % (name, value), text)
 
 
-def _configure(tmp, ni, nj, nt, nk, cfg):
+def _configure(tmp, ni, nj, nt, nk, cfg, usersource=None):
     """Copy the reference tree to tmp and select the model and run parameters
-    as `make ot` / `make fluxtube1` does; returns (src, inc)."""
+    as `make ot` / `make fluxtube1` does; returns (src, inc).  `usersource`
+    names a model whose user source term (models/usersource.cu.<model>)
+    replaces src/usersource.cu (built with -DUSE_USERSOURCE)."""
     three = nk is not None
     for d in ("src", "include", "models"):
         shutil.copytree(os.path.join(REFROOT, d), os.path.join(tmp, d))
@@ -95,6 +97,8 @@ def _configure(tmp, ni, nj, nt, nk, cfg):
         shutil.copy(os.path.join(mod, "usersource.cu." + model), os.path.join(src, "usersource.cu"))
         shutil.copy(os.path.join(mod, "initialisation_user.h.default"),
                     os.path.join(inc, "initialisation_user.h"))
+    if usersource:
+        shutil.copy(os.path.join(mod, "usersource.cu." + usersource), os.path.join(src, "usersource.cu"))
     ph = os.path.join(inc, "iosmaugparams.h")
     text = open(ph).read()
     text = _set_define(text, "NI", str(ni))
@@ -142,10 +146,15 @@ def _cached(name, stamp):
     return binp, stampf, fresh
 
 
-def build_ref(name, ni, nj, nt, arch="sm_100a", verbose=True, nk=None, defines=(), **kw):
+def build_ref(name, ni, nj, nt, arch="sm_100a", verbose=True, nk=None, defines=(), usersource=None,
+              **kw):
     """Build the reference's GPU binary for an ni x nj (x nk) grid and nt
     steps; `defines` are extra build macros of the reference (e.g.
-    USE_DORDER3, the 6th-order flux derivative), kw override iosmaugparams.h."""
+    USE_DORDER3, the 6th-order flux derivative), `usersource` a model whose
+    user source term is compiled in (models/usersource.cu.<model>, with
+    -DUSE_USERSOURCE), kw override iosmaugparams.h."""
+    if usersource:
+        defines = tuple(defines) + ("USE_USERSOURCE",)
     if not os.path.isdir(REFROOT):
         raise RuntimeError("reference sources not present at %s" % REFROOT)
     cfg = dict(DEFAULTS)
@@ -153,14 +162,15 @@ def build_ref(name, ni, nj, nt, arch="sm_100a", verbose=True, nk=None, defines=(
     three = nk is not None
     if three and nk > nj:
         raise ValueError("3D reference builds need nk <= nj")
-    stamp = "ni=%d nj=%d nk=%s nt=%d %s arch=%s%s\n" % (ni, nj, nk, nt, sorted(cfg.items()), arch,
-                                                     "".join(" -D" + d for d in defines))
+    stamp = "ni=%d nj=%d nk=%s nt=%d %s arch=%s%s%s\n" % (
+        ni, nj, nk, nt, sorted(cfg.items()), arch, "".join(" -D" + d for d in defines),
+        " usersource=%s" % usersource if usersource else "")
     binp, stampf, fresh = _cached(name, stamp)
     if fresh:
         return binp
     tmp = tempfile.mkdtemp(prefix="smaug_ref_")
     try:
-        src, inc = _configure(tmp, ni, nj, nt, nk, cfg)
+        src, inc = _configure(tmp, ni, nj, nt, nk, cfg, usersource)
         # workaround 1 (see module docstring)
         initcu = os.path.join(src, "init.cu")
         lines = open(initcu).read().split("\n")

@@ -70,7 +70,7 @@ class OracleRun:
         self.p = params
         self.pos, self.delx = grid_metric(params.ndim, list(params.n)[: params.ndim], pos)
         self.w = boundary(params, w)
-        self.state = np.array([params.dt, 0.0])
+        self.state = np.array([params.dt, 0.0, 0.0])  # dt, t, step counter
         self.cmax = np.zeros(3)
         self.it = 0
 

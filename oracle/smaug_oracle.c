@@ -68,6 +68,7 @@ typedef struct {
   double dt;             /* p->dt */
   double cmax;           /* p->cmax */
   double t;              /* simulated time, for the driver phase */
+  long it;               /* step counter (the reference's p->it = n) */
   int increment_mode;    /* slot1 starts at 0 for evolved fields (RK4 stages) */
 } O;
 
@@ -1014,8 +1015,16 @@ static double driver_v(const O *o, long c) {
   return v;
 }
 
+/* SMAUG_DRIVER_GAUSS_STEP: the reference's spicule1 model applies its term
+   only while p->it == 1 (models/usersource.cu.spicule1:67); p->it is the
+   step counter n of the driver loop (src/iosmaug.c:496-498), copied to the
+   device by cusource (src/centdiff2.cu:1229) */
 static void k_source(O *o) {
-  if (o->P->driver != SMAUG_DRIVER_GAUSS) return;
+  if (o->P->driver == SMAUG_DRIVER_GAUSS_STEP) {
+    if (o->it != o->P->drv_step) return;
+  } else if (o->P->driver != SMAUG_DRIVER_GAUSS) {
+    return;
+  }
   FOR_CELLS(o)
   double v = driver_v(o, _c);
   const double *wr = o->increment_mode ? o->w0 : o->w1;
@@ -1282,7 +1291,8 @@ int or_cmax(const smaug_params_t *P, const double *w, double *cmaxd) {
  * Advance `nsteps` steps.
  *   w      in/out, NVAR*dimp, the reference's slot 1 after boundaries (S_n)
  *   pos,delx geometry from or_grid_metric
- *   state  in/out: [0]=p->dt (previous dt), [1]=t (simulated time)
+ *   state  in/out: [0]=p->dt (previous dt), [1]=t (simulated time),
+ *          [2]=the step counter (p->it of the next step)
  *   cmax_out  per-dim CFL maxima of the last step input (may be NULL)
  * integrator: SMAUG_INT_EULER reproduces the reference step; SMAUG_INT_RK4
  * is classical RK4 on the same operator: dt from the CFL maxima of the step
@@ -1297,6 +1307,7 @@ int or_advance(const smaug_params_t *P, double *w, const double *pos,
   long nw = (long)o.nvar * o.dimp;
   double dtprev = state[0];
   o.t = state[1];
+  o.it = (long)state[2];
   double cmaxd[3] = {0, 0, 0};
   double *un = NULL, *acc = NULL, *ustage = NULL, *delta = NULL;
   if (P->integrator == SMAUG_INT_RK4) {
@@ -1320,6 +1331,7 @@ int or_advance(const smaug_params_t *P, double *w, const double *pos,
       memcpy(w, o.w1, sizeof(double) * nw);
       dtprev = o.dt;
       o.t += o.dt;
+      o.it++;
     } else {
       static const double cst[4] = {0.5, 0.5, 1.0, 0.0};
       static const double wgt[4] = {1.0 / 6.0, 1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0};
@@ -1362,12 +1374,14 @@ int or_advance(const smaug_params_t *P, double *w, const double *pos,
       memcpy(w, acc, sizeof(double) * nw);
       dtprev = dt;
       o.t = t0 + dt;
+      o.it++;
       continue;
     }
     if (cmax_out) memcpy(cmax_out, cmaxd, sizeof(double) * o.nd);
   }
   state[0] = dtprev;
   state[1] = o.t;
+  state[2] = (double)o.it;
 out:
   free(un); free(acc); free(ustage); free(delta);
   free_O(&o);

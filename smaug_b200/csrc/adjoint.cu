@@ -1073,6 +1073,8 @@ static int adj_create(const smaug_params_t* p, const double* w, const double* po
   if (p->precision != SMAUG_PREC_FP64) return set_error(SMAUG_E_UNSUPPORTED, "the adjoint is FP64");
   if (p->moddton != 0) return set_error(SMAUG_E_UNSUPPORTED, "the adjoint holds dt fixed: set moddton = 0");
   if (p->stencil_order == 6) return set_error(SMAUG_E_UNSUPPORTED, "the adjoint is of the 4th-order stencil");
+  if (p->driver == SMAUG_DRIVER_GAUSS_STEP)
+    return set_error(SMAUG_E_UNSUPPORTED, "the adjoint's driver acts in every step");
   if (p->n[0] < 8 || p->n[1] < 8) return set_error(SMAUG_E_INVALID, "grid too small");
   for (int d = 0; d < 2; d++) {
     const int b = p->boundtype[d][0];

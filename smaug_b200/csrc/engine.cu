@@ -259,7 +259,8 @@ static int validate(const smaug_params_t* p) {
   if (p->moddton == 1 && !(p->courant > 0))
     return set_error(SMAUG_E_INVALID, "courant must be > 0 with moddton");
   if (!(p->gamma > 1.0)) return set_error(SMAUG_E_INVALID, "gamma must be > 1");
-  if (p->driver != SMAUG_DRIVER_NONE && p->driver != SMAUG_DRIVER_GAUSS)
+  if (p->driver != SMAUG_DRIVER_NONE && p->driver != SMAUG_DRIVER_GAUSS &&
+      p->driver != SMAUG_DRIVER_GAUSS_STEP)
     return set_error(SMAUG_E_INVALID, "unknown driver %d", p->driver);
   if (p->stencil_order != 0 && p->stencil_order != 4 && p->stencil_order != 6)
     return set_error(SMAUG_E_INVALID, "stencil_order must be 4 or 6 (got %d)", p->stencil_order);
@@ -569,10 +570,15 @@ static int launch_stage(Engine* e, int mode, int stage, const void* uin, const v
                         const float* un_lo, void* uout, float* uout_lo) {
   KBufs B = fill_kbufs(e, mode, stage, e->parity, (int)(e->stage_count % 3), uin, un, un_lo, uout,
                        uout_lo);
+  // a driver that acts in one step only: the kernels see the plain Gaussian
+  // driver in that step and none in the others
+  KParams K = e->K;
+  if (K.driver == SMAUG_DRIVER_GAUSS_STEP)
+    K.driver = (e->it == e->P.drv_step) ? SMAUG_DRIVER_GAUSS : SMAUG_DRIVER_NONE;
   if (e->nd == 3)
-    CUDA_TRY(launch_stage3d_any(mode, e->mix, e->K, B, e->stream));
+    CUDA_TRY(launch_stage3d_any(mode, e->mix, K, B, e->stream));
   else
-    CUDA_TRY(launch_stage2d_any(mode, e->mix, e->K, B, e->stream));
+    CUDA_TRY(launch_stage2d_any(mode, e->mix, K, B, e->stream));
   e->stage_count++;
   return SMAUG_OK;
 }
@@ -993,6 +999,9 @@ static int batch_create(int nruns, const smaug_params_t* const* params, const do
       return fail(set_error(SMAUG_E_UNSUPPORTED, "run %d: all runs of a batch share one precision form", r));
     if (params[r]->stencil_order == 6)
       return fail(set_error(SMAUG_E_UNSUPPORTED, "run %d: batches use the 4th-order stencil", r));
+    if (params[r]->driver == SMAUG_DRIVER_GAUSS_STEP)
+      return fail(set_error(SMAUG_E_UNSUPPORTED, "run %d: batches replay steps; a one-step driver "
+                                                 "is not supported", r));
     Engine* e = nullptr;
     int rc = create(params[r], w[r], pos[r], &e);
     if (rc) return fail(rc);

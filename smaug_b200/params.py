@@ -28,6 +28,7 @@ PAD_ZERO = 1
 
 DRIVER_NONE = 0
 DRIVER_GAUSS = 1
+DRIVER_GAUSS_STEP = 2  # the same term in the step whose counter equals drv_step only
 
 
 class SmaugParams(ctypes.Structure):
@@ -43,7 +44,8 @@ class SmaugParams(ctypes.Structure):
         ("boundtype", (ctypes.c_int32 * 2) * 3),
         ("driver", ctypes.c_int32),
         ("stencil_order", ctypes.c_int32),
-        ("reserved_i", ctypes.c_int32 * 6),
+        ("drv_step", ctypes.c_int32),
+        ("reserved_i", ctypes.c_int32 * 5),
         ("dx", ctypes.c_double * 3),
         ("dt", ctypes.c_double),
         ("dtmax", ctypes.c_double),
@@ -112,7 +114,8 @@ def make_params(ndim=2, n=(132, 132, 1), dx=None, gamma=5.0 / 3.0, courant=0.3,
                 boundtype=None, integrator=INT_EULER, g=(0.0, 0.0, 0.0),
                 eta=0.0, xmin=(0.0, 0.0, 0.0), pad_model=PAD_STRAY,
                 driver=DRIVER_NONE, drv_amp=0.0, drv_period=0.0, precision=PREC_FP64,
-                drv_x0=(0.0, 0.0, 0.0), drv_sigma=(0.0, 0.0, 0.0), stencil_order=4):
+                drv_x0=(0.0, 0.0, 0.0), drv_sigma=(0.0, 0.0, 0.0), stencil_order=4,
+                drv_step=0):
     """Build a parameter block.  Defaults: the reference's Orszag-Tang model
     (models/iosmaugparams.h.ot) with a 0.3 Courant number; `chyp` may be a
     scalar (every field) or a sequence indexed by field; stencil_order 6
@@ -160,4 +163,5 @@ def make_params(ndim=2, n=(132, 132, 1), dx=None, gamma=5.0 / 3.0, courant=0.3,
     p.stencil_order = stencil_order
     p.drv_amp = drv_amp
     p.drv_period = drv_period
+    p.drv_step = drv_step
     return p

@@ -93,6 +93,54 @@ CASES3 = {
 
 # the reference built with -DUSE_DORDER3 (same tuple layouts as CASES / CASES3)
 CASES_O6 = {"d16": (16, 16, 15, 21, [1, 2, 3, 5, 10, 20])}
+
+# The user source term of the reference's spicule1 model
+# (models/usersource.cu.spicule1:3-137, built with -DUSE_USERSOURCE into the
+# Orszag-Tang build): m_1 += dt vvz (rho + rho_b) with
+# vvz = 200 exp(-(z-xc1)^2/dz^2) exp(-(x-xc2)^2/dx^2), z = xmin_0 + i dx_0,
+# x = xmin_1 + j dx_1 (ghosts included), xc1 = 0.0174 Mm, xc2 = 1.998046 Mm,
+# dz = dx = 1 km, applied in the step whose counter p->it is 1 only.  The
+# domain is placed around the driver's centre in metres with 1 km cells, so
+# that the term reaches several cells: dim 0 [8, 26] km, dim 1
+# [1990, 2008] km, 18 x 18 interior cells (one thread block: race-free).  The
+# state is an Orszag-Tang pattern in solar units with a uniform background
+# density and pressure (energyb) and positions equal to the source's own
+# z and x, so that the engine's Gaussian driver with the same centre and
+# width reproduces the term.
+# name: (nx, ny, seed, NT, steps kept)
+CASES_DRV = {"s18": (18, 18, 31, 11, [1, 2, 3, 5, 10])}
+DRV_DOMAIN = (8.0e3, 26.0e3, 1.99e6, 2.008e6)        # XMIN XMAX YMIN YMAX [m]
+DRV_PARAMS = {"drv_amp": 200.0, "drv_period": 0.0, "drv_step": 1,
+              "drv_x0": (0.0174 * 1.0e6, 1.998046 * 1.0e6), "drv_sigma": (0.001e6, 0.001e6)}
+
+
+def spicule_state(nx, ny, seed, gamma=GAMMA_REF):
+    """Orszag-Tang pattern in solar units on DRV_DOMAIN: total density
+    2.7e-4 kg/m^3 (2e-4 of it background), flow 1 km/s, gas pressure 1.6e4 Pa
+    (1.2e4 of it background, as energyb), field 82 (SAC units); positions
+    xmin + i dx including ghosts, as the spicule1 source computes them."""
+    x0, x1, y0, y1 = DRV_DOMAIN
+    dx, dy = (x1 - x0) / nx, (y1 - y0) / ny
+    X = x0 + np.arange(nx + 4) * dx
+    Y = y0 + np.arange(ny + 4) * dy
+    Xg, Yg = np.meshgrid(X, Y, indexing="xy")
+    xs = 2 * math.pi * (Xg - (x0 - 1.5 * dx)) / (x1 - x0)
+    ys = 2 * math.pi * (Yg - (y0 - 1.5 * dy)) / (y1 - y0)
+    rng = np.random.default_rng(seed)
+    rhob = 2.0e-4
+    rho = 0.7e-4 * (1 + 1e-3 * rng.standard_normal(Xg.shape))
+    rt = rho + rhob
+    b0 = 82.0
+    w = np.zeros((10,) + Xg.shape)
+    w[0] = rho
+    w[1] = -rt * 1.0e3 * np.sin(ys)
+    w[2] = rt * 1.0e3 * np.sin(xs)
+    w[4] = -b0 * np.sin(ys)
+    w[5] = b0 * np.sin(2 * xs)
+    w[3] = 0.4e4 / (gamma - 1) + 0.5 * (w[1] ** 2 + w[2] ** 2) / rt + 0.5 * (w[4] ** 2 + w[5] ** 2)
+    w[6] = 1.2e4 / (gamma - 1)
+    w[7] = rhob
+    return w, np.stack([Xg, Yg]), (dx, dy)
 CASES3_O6 = {"d3s": ((4, 4, 4), 25, 21, [1, 2, 3, 5, 10, 20], 1)}
 O6 = ("USE_DORDER3",)
 
@@ -192,6 +240,14 @@ def prepare():
             formats.write_ini(os.path.join(WORK, name + ".ini"), w, pos)
             build_ref.build_ref(name, nx, ny, nt, verbose=False, defines=defines, **_bc_defines(case))
             print("prepared", name)
+    for name, case in _selected(CASES_DRV).items():
+        nx, ny, seed, nt, keep = case
+        w, pos, _ = spicule_state(nx, ny, seed)
+        formats.write_ini(os.path.join(WORK, name + ".ini"), w, pos)
+        x0, x1, y0, y1 = DRV_DOMAIN
+        build_ref.build_ref(name, nx, ny, nt, verbose=False, usersource="spicule1",
+                            XMIN=repr(x0), XMAX=repr(x1), YMIN=repr(y0), YMAX=repr(y1))
+        print("prepared", name)
     for table, defines in ((CASES3, ()), (CASES3_O6, O6)):
         for name, case in _selected(table).items():
             (nx, ny, nz), seed, nt, keep, runs = case[:5]
@@ -227,7 +283,7 @@ def _bc_defines(case):
 
 
 def run():
-    for name, case in _selected({**CASES, **CASES_O6}).items():
+    for name, case in _selected({**CASES, **CASES_O6, **CASES_DRV}).items():
         _run_one(name, case[4])
         if name in TWICE:
             _run_one(name, case[4], "_r1")
@@ -255,6 +311,22 @@ def collect():
                             hdr_t=np.array(times), gamma=GAMMA_REF,
                             dx=np.array([L3 / nx, L3 / ny, L3 / nz]),
                             g=np.array([G3, 0.0, 0.0]), **extra)
+        print("wrote", name)
+    for name, case in _selected(CASES_DRV).items():
+        nx, ny, seed, nt, keep = case
+        w0, pos0, _ = formats.read_ini(os.path.join(WORK, name + ".ini"), 2)
+        states, times = [], []
+        for k in keep:
+            w, pos, h = formats.read_out(os.path.join(RUNS, name, "out", "ref_%d.out" % k))
+            states.append(w)
+            times.append(h["t"])
+        _, _, dx = spicule_state(nx, ny, seed)
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), w0=w0, pos=pos0,
+                            steps=np.array(keep), states=np.array(states),
+                            hdr_t=np.array(times), gamma=GAMMA_REF, dx=np.array(dx),
+                            drv_amp=DRV_PARAMS["drv_amp"], drv_step=DRV_PARAMS["drv_step"],
+                            drv_x0=np.array(DRV_PARAMS["drv_x0"]),
+                            drv_sigma=np.array(DRV_PARAMS["drv_sigma"]))
         print("wrote", name)
     for name, case in _selected({**CASES, **CASES_O6}).items():
         nx, ny, seed, nt, keep = case[:5]

@@ -13,12 +13,13 @@ RACE = ("ot128",)                      # 128^2, 200 steps, two runs of the refer
 STRICT3 = ("t3s", "t3a", "t3b", "t3f")  # 3D flux-tube build, contcd4 (t3f: fixed dim 0) ghosts
 ORDER6 = ("d16",)                      # 2D, the reference built with -DUSE_DORDER3
 ORDER6_3D = ("d3s",)                   # 3D, the same
+DRIVER = ("s18",)                      # 2D, the spicule1 model's user source term
 
 
 def load(name):
     z = np.load(os.path.join(GOLDEN, name + ".npz"))
     d = {k: z[k] for k in z.files}
-    if d["w0"].ndim == 4:          # 3D fixtures hold all 13 fields
+    if d["w0"].ndim == 4 or d["w0"].shape[0] == 10:  # all fields (3D; 2D with backgrounds)
         d["w0full"] = d["w0"].copy()
         return d
     w0 = np.zeros((10,) + d["w0"].shape[1:])
@@ -39,6 +40,12 @@ def params(d, **kw):
                              gamma=float(d["gamma"]), courant=0.3, dtmax=1.0, dt=1e-8,
                              g=tuple(d["g"]), **kw)
     ny, nx = d["w0"].shape[1:]
+    if "drv_amp" in d:
+        kw.setdefault("driver", P.DRIVER_GAUSS_STEP)
+        kw.setdefault("drv_amp", float(d["drv_amp"]))
+        kw.setdefault("drv_step", int(d["drv_step"]))
+        kw.setdefault("drv_x0", tuple(float(v) for v in d["drv_x0"]))
+        kw.setdefault("drv_sigma", tuple(float(v) for v in d["drv_sigma"]))
     if "bt" in d:
         kw.setdefault("boundtype", tuple(int(b) for b in d["bt"]))
     return P.make_params(ndim=2, n=(nx, ny, 1), dx=tuple(d["dx"]), gamma=float(d["gamma"]),

@@ -13,7 +13,7 @@ from tests.util import rel_l2
 TOL = 1e-13
 
 
-@pytest.mark.parametrize("name", G.STRICT + G.BOUNDARY + G.ORDER6)
+@pytest.mark.parametrize("name", G.STRICT + G.BOUNDARY + G.ORDER6 + G.DRIVER)
 def test_oracle_matches_reference_run(oracle, name):
     d = G.load(name)
     p = G.params(d)
@@ -72,6 +72,19 @@ def test_zero_pad_model_does_not_match(oracle):
     p = G.params(d, pad_model=P.PAD_ZERO)
     run = oracle.OracleRun(p, d["w0full"], d["pos"]).advance(1)
     assert max(rel_l2(run.w[f], d["states"][0][f]) for f in range(6)) > 1e-8
+
+
+def test_driver_term_matters(oracle):
+    """The spicule1 source term is seen by the fixture: the reference's state
+    after its kicked step (p->it == 1) differs from an undriven run, from a
+    run driven in every step and from one kicked a step late."""
+    from smaug_b200 import params as P
+    d = G.load("s18")
+    assert int(d["steps"][1]) == 2  # the state after the step with counter 1
+    ref = d["states"][1]
+    for kw in ({"driver": P.DRIVER_NONE}, {"driver": P.DRIVER_GAUSS}, {"drv_step": 2}):
+        run = oracle.OracleRun(G.params(d, **kw), d["w0full"], d["pos"]).advance(2)
+        assert rel_l2(run.w[1], ref[1]) > 1e-6, kw
 
 
 @pytest.mark.parametrize("name", G.RACE)
