@@ -2,7 +2,7 @@
 //
 // One fused kernel per stage evaluates the whole spatial operator of the
 // reference's single-stage step (src/iosmaug.c:631-835) for a 2D tile
-// (stage2d.cuh) or a z-marching 3D column (stage3d_zm.cuh):
+// (stage2d.cuh) or a 3D tile (stage3d.cuh):
 //   state tile + 3-cell halo staged in shared memory
 //   -> directional fluxes + 4th-order divergence     (src/centdiff1.cu, centdiff2.cu)
 //   -> background energy coupling, gravity            (src/centdiff2.cu:80-154)

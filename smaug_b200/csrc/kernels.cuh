@@ -301,17 +301,6 @@ cudaError_t launch_stage3d_any(int mode, bool mix, const KParams& K, const KBufs
 cudaError_t stage2d_set_attributes();
 cudaError_t stage3d_set_attributes();
 
-// the z-marching 3D stage kernel per integrator and precision form
-// (stage3d_zm_*.cu); nsm = SM count of the device (chooses the z-chunk)
-#define SMAUG_ZM_DECL(NAME)                                                                   \
-  cudaError_t zm_launch_##NAME(const KParams& K, const KBufs& B, cudaStream_t st, int nsm);   \
-  cudaError_t zm_attr_##NAME();
-SMAUG_ZM_DECL(euler_fp64)
-SMAUG_ZM_DECL(euler_mixed)
-SMAUG_ZM_DECL(rk4_fp64)
-SMAUG_ZM_DECL(rk4_mixed)
-#undef SMAUG_ZM_DECL
-
 // batched 2D stages (batch_kernel.cuh), one instantiation per tile shape
 // (batch.cu: 32x8, batch16.cu: 16x16): Ks/Bs per run in device memory,
 // tiles = (run, tile x, tile y) work list of that shape, `grid` persistent
