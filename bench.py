@@ -56,10 +56,25 @@ METRIC = "Mcell-updates/s per RK4 step"
 UNIT = "Mcell-updates/s"
 
 
-# DRAM bytes per interior cell per RK4 step measured by ncu on all four stage
-# launches (profiles/dram_traffic_per_stage.md: 2D at 2048^2, 3D at 128^3)
-TRAFFIC_PER_CELL_STEP = {(2, "fp64"): 865.8, (2, "mixed"): 723.8, (3, "fp64"): 1482.3,
-                         (3, "mixed"): 1230.8}
+# DRAM bytes per interior cell per RK4 step measured by ncu on the four stage
+# launches of one step at the benchmark sizes (profiles/dram_traffic_per_stage.md:
+# 2D at 4096^2, 3D at 256^3)
+TRAFFIC_PER_CELL_STEP = {(2, "fp64"): 889.1, (2, "mixed"): 745.7, (3, "fp64"): 2241.6,
+                         (3, "mixed"): 1510.6}
+
+# What bounds each stage kernel, from its ncu section set (profiles/)
+BOUND_NOTE = {
+    (2, "fp64"): "issue-bound, not HBM: 109 warp instructions per cell and stage at 59.8 % issue "
+                 "active, FP64 pipe 35 %, barrier stalls 2.9 per issue "
+                 "(profiles/stage2d_fp64_ot2048_full.md)",
+    (2, "mixed"): "issue-bound, not HBM: 102 warp instructions per cell and stage at 60.5 % issue "
+                  "active (profiles/stage2d_mixed_ot2048_full.md)",
+    (3, "fp64"): "latency/issue-bound, not HBM: 494 warp instructions per cell and stage at 47.8 % "
+                 "issue active, long-scoreboard stalls 3.65 per issue from re-reads of the state, "
+                 "DRAM traffic 1.8x the algorithmic bytes (profiles/stage3d_fp64_tube128_full.md)",
+    (3, "mixed"): "latency/issue-bound, not HBM: as the FP64 form, with float storage "
+                  "(profiles/stage3d_fp64_tube128_full.md)",
+}
 
 # FP64 (and FP32) floating-point operations per interior cell per stage counted
 # by ncu (smsp__sass_thread_inst_executed_op_{dadd,dmul,dfma}_pred_on, an FMA
@@ -111,6 +126,26 @@ def scheme_bytes_per_cell_step(ndim, mixed=False):
     3D: 1184); mixed 100P+32B (2D: 728, 3D: 960)."""
     P, B = 2 + 2 * ndim, 2 + ndim
     return 100 * P + 32 * B if mixed else (16 * P + 4 * B) * 8
+
+
+def roofline_block(ndim, prec, alg_bytes, ncell, steps, ms, peak, peak_kind):
+    """HBM roofline of the stage kernel: achieved = algorithmic bytes per
+    interior cell and step x cells x steps / device time; traffic = the DRAM
+    bytes ncu measured per stage launch at this size, and the bandwidth the
+    kernel actually drew from them (achieved_by_traffic)."""
+    achieved = alg_bytes * ncell * steps / (ms / 1e3) / 1e9
+    tcell = TRAFFIC_PER_CELL_STEP.get((ndim, prec))
+    out = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+           "peak_kind": peak_kind, "alg_bytes_per_cell_step": alg_bytes,
+           "scheme_bytes_per_cell_step": scheme_bytes_per_cell_step(ndim, prec == "mixed"),
+           "traffic": tcell * ncell / 4 if tcell else None,
+           "traffic_unit": "DRAM bytes per stage launch (ncu at the benchmark size)",
+           "note": BOUND_NOTE.get((ndim, prec))}
+    if tcell:
+        by_traffic = tcell * ncell * steps / (ms / 1e3) / 1e9
+        out["achieved_by_traffic"] = by_traffic
+        out["frac_by_traffic"] = by_traffic / peak
+    return out
 
 
 def peaks():
@@ -851,15 +886,12 @@ def main():
                  "speedup_vs_fp64": mval / value, "dtype": "f32 storage + hyperdiffusion, f64 rest",
                  "rel_l2_vs_fp64": {"steps": args.warmup + args.steps, "max": max(errs),
                                     "per_field": errs},
-                 "roofline": {"bound": "hbm", "achieved": mach, "peak": peak_m, "unit": "GB/s",
-                              "frac": mach / peak_m, "alg_bytes_per_cell_step": mbytes,
-                              "scheme_bytes_per_cell_step": scheme_bytes_per_cell_step(p.ndim, True),
-                              "traffic": TRAFFIC_PER_CELL_STEP[(p.ndim, "mixed")] * ncell_int / 4},
+                 "roofline": roofline_block(p.ndim, "mixed", mbytes, ncell_int, args.steps, mms, peak_m,
+                                            peaks()[1]),
                  "fp64_roofline": fp64_roofline(p.ndim, "mixed", ncell_int, args.steps, mms)}
 
     if rank == 0:
         peak, pk_kind = peaks()
-        achieved = alg_bytes * ncell_int * args.steps / (ms / 1e3) / 1e9
         state_gb = (2 + 2 * p.ndim) * p.ncells * 8 / 1e9
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws,
@@ -876,15 +908,8 @@ def main():
                     "path": "smaug_set_state + smaug_step + smaug_get_fields (evolved fields), pinned host buffers",
                     "gpu_launches_per_step": 4 + 2},
             "gpu_launches": launches,
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak,
-                         "traffic": TRAFFIC_PER_CELL_STEP.get((p.ndim, args.precision), 0.0)
-                         * ncell_int / 4 or None,
-                         "traffic_unit": "bytes per stage launch (ncu, scaled by cells)",
-                         "peak_kind": pk_kind,
-                         "alg_bytes_per_cell_step": alg_bytes,
-                         "scheme_bytes_per_cell_step": scheme_bytes_per_cell_step(p.ndim),
-                         "note": "stage kernel; FP64 arithmetic, not HBM, limits this form"},
+            "roofline": roofline_block(p.ndim, args.precision, alg_bytes, ncell_int, args.steps, ms,
+                                       peak, pk_kind),
             "fp64_roofline": fp64_roofline(p.ndim, args.precision, ncell_int, args.steps, ms_max),
             "clocks": clk.summary(),
             "mixed": mixed,

@@ -115,6 +115,10 @@ def _configure(tmp, ni, nj, nt, nk, cfg, usersource=None):
     for k in ("BCU0", "BCL0", "BCU1", "BCL1") + (("BCU2", "BCL2") if three else ()):
         if k in cfg:
             text = _set_define(text, k, cfg[k])
+    if not three:  # 2D gravity, when given (models/iosmaugparams.h.ot:17-19)
+        for k in ("PGRAV0", "PGRAV1"):
+            if k in cfg:
+                text = _set_define(text, k, cfg[k])
     for k in ("PCHYP", "PCHYPRHO", "PCHYPENERGY", "PCHYPB0", "PCHYPB1", "PCHYPB2",
               "PCHYPMOM0", "PCHYPMOM1", "PCHYPMOM2"):
         text = _set_define(text, k, cfg.get(k, cfg["CHYP"]))

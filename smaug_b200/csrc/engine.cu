@@ -180,6 +180,7 @@ struct Engine {
   int parity = 0;                        // dt/t double buffer
   int64_t it = 0;
   int device = 0;
+  bool ghost_upd = false;                // 2D fixed ghost layers updated every stage
   cudaStream_t own_stream = nullptr;     // created by the engine
   Snapshot snap[2];                      // asynchronous .out writes, used in turn
   int snap_next = 0;
@@ -252,9 +253,11 @@ static int validate(const smaug_params_t* p) {
         b != SMAUG_BC_ASYMM && b != SMAUG_BC_FIXED)
       return set_error(SMAUG_E_UNSUPPORTED, "dim %d: boundary type %d not supported", d, b);
     // the reference adds the driver term to every cell, ghosts included
-    // (src/centdiff2.cu:790-872); only fixed ghost cells would keep it
-    if (b == SMAUG_BC_FIXED && p->driver != SMAUG_DRIVER_NONE)
-      return set_error(SMAUG_E_UNSUPPORTED, "dim %d: fixed boundaries with a driver term", d);
+    // (src/centdiff2.cu:790-872), and fixed ghost cells keep it; the 2D
+    // engine updates its fixed ghost layers as the reference does
+    // (fixed_ghost2d_kernel), the 3D one does not
+    if (b == SMAUG_BC_FIXED && p->driver != SMAUG_DRIVER_NONE && p->ndim == 3)
+      return set_error(SMAUG_E_UNSUPPORTED, "dim %d: 3D fixed boundaries with a driver term", d);
   }
   if (p->moddton == 1 && !(p->courant > 0))
     return set_error(SMAUG_E_INVALID, "courant must be > 0 with moddton");
@@ -382,16 +385,19 @@ static int create(const smaug_params_t* p, const double* w, const double* pos, E
   for (int f = 2 + 2 * e->nd; f < nvar && !K.has_bg; f++)
     for (long c = 0; c < nc; c++)
       if (w[(size_t)f * nc + c] != 0.0) { K.has_bg = 1; break; }
-  // The reference's 2D gravity (src/centdiff2.cu:721-787) and background
-  // energy coupling (src/centdiff2.cu:587-717) also update ghost cells; with
-  // fixed boundaries nothing overwrites them there, so those ghost layers
-  // drift.  The engine keeps fixed ghost cells constant, which agrees with
-  // the reference only without both terms.  (Its 3D kernels stay interior.)
-  if (e->nd == 2 && has_fixed(K) && (K.has_bg || K.has_grav)) {
+  // The reference's 2D gravity (src/centdiff2.cu:721-787), background
+  // energy coupling (src/centdiff2.cu:587-717) and driver (every cell) also
+  // update ghost cells, and fixed boundaries never overwrite them there: the
+  // fixed ghost layers drift.  fixed_ghost2d_kernel reproduces that after
+  // every 2D stage; the 3D kernels stay interior and 3D fixed boundaries with
+  // these terms match the reference (its 3D kernels are bounded to the
+  // interior).
+  e->ghost_upd = e->nd == 2 && has_fixed(K) && (K.has_bg || K.has_grav || p->driver != SMAUG_DRIVER_NONE);
+  if (e->ghost_upd && p->stencil_order == 6) {
     delete e;
     return set_error(SMAUG_E_UNSUPPORTED,
-                     "2D fixed boundaries with gravity or background fields: the reference also "
-                     "updates those ghost layers");
+                     "2D fixed boundaries with gravity, background fields or a driver use the "
+                     "4th-order stencil");
   }
   K.driver = p->driver;
   K.drv_amp = p->drv_amp;
@@ -519,6 +525,12 @@ static int reset_derived(Engine* e) {
         CUDA_TRY(cudaMemcpyAsync(e->d_h[3], e->d_h[2], sizeof(float) * n, cudaMemcpyDeviceToDevice,
                                  e->stream));
     }
+    if (e->ghost_upd) {
+      // the fixed ghost layers change: fixed_ghost2d_kernel adds their CFL
+      // speeds to every stage's maxima, so there is no constant floor
+      for (int d = 0; d < 3; d++) e->K.cmax_floor[d] = 0.0;
+      return SMAUG_OK;
+    }
     unsigned long long* fl = e->d_cmax + 9;
     CUDA_TRY(cudaMemsetAsync(fl, 0, sizeof(unsigned long long) * 3, e->stream));
     if (e->nd == 3)
@@ -575,10 +587,12 @@ static int launch_stage(Engine* e, int mode, int stage, const void* uin, const v
   KParams K = e->K;
   if (K.driver == SMAUG_DRIVER_GAUSS_STEP)
     K.driver = (e->it == e->P.drv_step) ? SMAUG_DRIVER_GAUSS : SMAUG_DRIVER_NONE;
-  if (e->nd == 3)
+  if (e->nd == 3) {
     CUDA_TRY(launch_stage3d_any(mode, e->mix, K, B, e->stream));
-  else
+  } else {
     CUDA_TRY(launch_stage2d_any(mode, e->mix, K, B, e->stream));
+    if (e->ghost_upd) CUDA_TRY(launch_fixed_ghost2d(mode, e->mix, K, B, e->stream));
+  }
   e->stage_count++;
   return SMAUG_OK;
 }
@@ -1006,6 +1020,9 @@ static int batch_create(int nruns, const smaug_params_t* const* params, const do
     int rc = create(params[r], w[r], pos[r], &e);
     if (rc) return fail(rc);
     b->runs.push_back(e);
+    if (e->ghost_upd)
+      return fail(set_error(SMAUG_E_UNSUPPORTED, "run %d: batches keep fixed ghost layers constant; "
+                                                 "gravity, background fields or a driver update them", r));
     rc = reset_derived(e);
     if (rc) return fail(rc);
   }

@@ -300,6 +300,8 @@ cudaError_t launch_stage2d_any(int mode, bool mix, const KParams& K, const KBufs
 cudaError_t launch_stage3d_any(int mode, bool mix, const KParams& K, const KBufs& B, cudaStream_t st);
 cudaError_t stage2d_set_attributes();
 cudaError_t stage3d_set_attributes();
+// the fixed ghost layers of a 2D stage, after the stage launch (stage2d.cu)
+cudaError_t launch_fixed_ghost2d(int mode, bool mix, const KParams& K, const KBufs& B, cudaStream_t st);
 
 // batched 2D stages (batch_kernel.cuh), one instantiation per tile shape
 // (batch.cu: 32x8, batch16.cu: 16x16): Ks/Bs per run in device memory,

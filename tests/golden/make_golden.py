@@ -107,19 +107,47 @@ CASES_O6 = {"d16": (16, 16, 15, 21, [1, 2, 3, 5, 10, 20])}
 # density and pressure (energyb) and positions equal to the source's own
 # z and x, so that the engine's Gaussian driver with the same centre and
 # width reproduces the term.
-# name: (nx, ny, seed, NT, steps kept)
-CASES_DRV = {"s18": (18, 18, 31, 11, [1, 2, 3, 5, 10])}
-DRV_DOMAIN = (8.0e3, 26.0e3, 1.99e6, 2.008e6)        # XMIN XMAX YMIN YMAX [m]
+# fs18: the same with fixed (5) ghosts along dim 0 and the domain moved so
+# that the driver's centre lies on ghost column 1: the reference's driver acts
+# on every cell, and a fixed boundary keeps the ghost values it leaves.
+# name: (nx, ny, seed, NT, steps kept, XMIN XMAX YMIN YMAX [m], boundary types)
+DRV_DOMAIN = (8.0e3, 26.0e3, 1.99e6, 2.008e6)
+CASES_DRV = {"s18": (18, 18, 31, 11, [1, 2, 3, 5, 10], DRV_DOMAIN, (0, 0)),
+             "fs18": (18, 18, 33, 11, [1, 2, 3, 5, 10], (16.4e3, 34.4e3, 1.99e6, 2.008e6), (5, 0))}
+
+# Fixed (5) ghosts together with gravity and background fields: the OT build
+# with PGRAV0/1 set and nonzero energyb, rhob, b1b, b2b in the .ini.  The
+# reference's 2D gravity and energy-coupling kernels also update the two low
+# ghost layers (src/centdiff2.cu:587-787), which the fixed boundary keeps.
+# name: (nx, ny, seed, NT, steps kept, boundary types, gravity)
+CASES_FG = {"fg16": (16, 16, 41, 21, [1, 2, 3, 5, 10, 20], (5, 0), (0.2, -0.1)),
+            "fg18y": (18, 12, 42, 21, [1, 2, 3, 5, 10, 20], (0, 5), (-0.1, 0.15))}
+
+
+def ot_background_state(nx, ny, seed):
+    """ot_state plus smooth nonzero background fields with the same total
+    state (rho_b, e_b moved out of rho, e)."""
+    w, pos = ot_state(nx, ny, seed)
+    n1, n0 = w.shape[1:]
+    jj, ii = np.meshgrid(np.arange(n1), np.arange(n0), indexing="ij")
+    rb = 0.1 * (1 + 0.2 * np.sin(2 * math.pi * ii / n0))
+    w[7] = rb
+    w[0] = w[0] - rb
+    w[8] = 0.05 * np.cos(2 * math.pi * jj / n1)
+    w[9] = 0.025
+    w[6] = 0.05 + 0.01 * np.cos(2 * math.pi * ii / n0)
+    w[3] = w[3] - w[6]
+    return w, pos
 DRV_PARAMS = {"drv_amp": 200.0, "drv_period": 0.0, "drv_step": 1,
               "drv_x0": (0.0174 * 1.0e6, 1.998046 * 1.0e6), "drv_sigma": (0.001e6, 0.001e6)}
 
 
-def spicule_state(nx, ny, seed, gamma=GAMMA_REF):
-    """Orszag-Tang pattern in solar units on DRV_DOMAIN: total density
+def spicule_state(nx, ny, seed, gamma=GAMMA_REF, domain=DRV_DOMAIN):
+    """Orszag-Tang pattern in solar units on `domain`: total density
     2.7e-4 kg/m^3 (2e-4 of it background), flow 1 km/s, gas pressure 1.6e4 Pa
     (1.2e4 of it background, as energyb), field 82 (SAC units); positions
     xmin + i dx including ghosts, as the spicule1 source computes them."""
-    x0, x1, y0, y1 = DRV_DOMAIN
+    x0, x1, y0, y1 = domain
     dx, dy = (x1 - x0) / nx, (y1 - y0) / ny
     X = x0 + np.arange(nx + 4) * dx
     Y = y0 + np.arange(ny + 4) * dy
@@ -241,12 +269,20 @@ def prepare():
             build_ref.build_ref(name, nx, ny, nt, verbose=False, defines=defines, **_bc_defines(case))
             print("prepared", name)
     for name, case in _selected(CASES_DRV).items():
-        nx, ny, seed, nt, keep = case
-        w, pos, _ = spicule_state(nx, ny, seed)
+        nx, ny, seed, nt, keep, dom, bt = case
+        w, pos, _ = spicule_state(nx, ny, seed, domain=dom)
         formats.write_ini(os.path.join(WORK, name + ".ini"), w, pos)
-        x0, x1, y0, y1 = DRV_DOMAIN
+        x0, x1, y0, y1 = dom
         build_ref.build_ref(name, nx, ny, nt, verbose=False, usersource="spicule1",
-                            XMIN=repr(x0), XMAX=repr(x1), YMIN=repr(y0), YMAX=repr(y1))
+                            XMIN=repr(x0), XMAX=repr(x1), YMIN=repr(y0), YMAX=repr(y1),
+                            **_bc_defines(case[:5] + (bt,)))
+        print("prepared", name)
+    for name, case in _selected(CASES_FG).items():
+        nx, ny, seed, nt, keep, bt, g = case
+        w, pos = ot_background_state(nx, ny, seed)
+        formats.write_ini(os.path.join(WORK, name + ".ini"), w, pos)
+        build_ref.build_ref(name, nx, ny, nt, verbose=False, PGRAV0=repr(g[0]), PGRAV1=repr(g[1]),
+                            **_bc_defines(case[:5] + (bt,)))
         print("prepared", name)
     for table, defines in ((CASES3, ()), (CASES3_O6, O6)):
         for name, case in _selected(table).items():
@@ -283,7 +319,7 @@ def _bc_defines(case):
 
 
 def run():
-    for name, case in _selected({**CASES, **CASES_O6, **CASES_DRV}).items():
+    for name, case in _selected({**CASES, **CASES_O6, **CASES_DRV, **CASES_FG}).items():
         _run_one(name, case[4])
         if name in TWICE:
             _run_one(name, case[4], "_r1")
@@ -312,21 +348,28 @@ def collect():
                             dx=np.array([L3 / nx, L3 / ny, L3 / nz]),
                             g=np.array([G3, 0.0, 0.0]), **extra)
         print("wrote", name)
-    for name, case in _selected(CASES_DRV).items():
-        nx, ny, seed, nt, keep = case
+    for name, case in _selected({**CASES_DRV, **CASES_FG}).items():
+        nx, ny, seed, nt, keep = case[:5]
         w0, pos0, _ = formats.read_ini(os.path.join(WORK, name + ".ini"), 2)
         states, times = [], []
         for k in keep:
             w, pos, h = formats.read_out(os.path.join(RUNS, name, "out", "ref_%d.out" % k))
             states.append(w)
             times.append(h["t"])
-        _, _, dx = spicule_state(nx, ny, seed)
+        if name in CASES_DRV:
+            dom, bt = case[5], case[6]
+            _, _, dx = spicule_state(nx, ny, seed, domain=dom)
+            extra = dict(drv_amp=DRV_PARAMS["drv_amp"], drv_step=DRV_PARAMS["drv_step"],
+                         drv_x0=np.array(DRV_PARAMS["drv_x0"]),
+                         drv_sigma=np.array(DRV_PARAMS["drv_sigma"]))
+        else:
+            bt, g = case[5], case[6]
+            dx = (2 * math.pi / nx, 2 * math.pi / ny)
+            extra = dict(g=np.array(g))
         np.savez_compressed(os.path.join(HERE, name + ".npz"), w0=w0, pos=pos0,
                             steps=np.array(keep), states=np.array(states),
                             hdr_t=np.array(times), gamma=GAMMA_REF, dx=np.array(dx),
-                            drv_amp=DRV_PARAMS["drv_amp"], drv_step=DRV_PARAMS["drv_step"],
-                            drv_x0=np.array(DRV_PARAMS["drv_x0"]),
-                            drv_sigma=np.array(DRV_PARAMS["drv_sigma"]))
+                            bt=np.array(bt), **extra)
         print("wrote", name)
     for name, case in _selected({**CASES, **CASES_O6}).items():
         nx, ny, seed, nt, keep = case[:5]

@@ -14,6 +14,9 @@ STRICT3 = ("t3s", "t3a", "t3b", "t3f")  # 3D flux-tube build, contcd4 (t3f: fixe
 ORDER6 = ("d16",)                      # 2D, the reference built with -DUSE_DORDER3
 ORDER6_3D = ("d3s",)                   # 3D, the same
 DRIVER = ("s18",)                      # 2D, the spicule1 model's user source term
+# 2D fixed ghosts that the reference updates: gravity and background fields
+# (fg16 fixed along dim 0, fg18y along dim 1), the driver (fs18)
+FIXED_UPDATES = ("fg16", "fg18y", "fs18")
 
 
 def load(name):
@@ -48,6 +51,8 @@ def params(d, **kw):
         kw.setdefault("drv_sigma", tuple(float(v) for v in d["drv_sigma"]))
     if "bt" in d:
         kw.setdefault("boundtype", tuple(int(b) for b in d["bt"]))
+    if "g" in d:
+        kw.setdefault("g", tuple(float(v) for v in d["g"]))
     return P.make_params(ndim=2, n=(nx, ny, 1), dx=tuple(d["dx"]), gamma=float(d["gamma"]),
                          courant=0.3, dtmax=1.0, dt=1e-8, **kw)
 

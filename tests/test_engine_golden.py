@@ -10,7 +10,7 @@ pytestmark = pytest.mark.gpu
 TOL = 1e-13
 
 
-@pytest.mark.parametrize("name", G.STRICT + G.BOUNDARY + G.ORDER6 + G.DRIVER)
+@pytest.mark.parametrize("name", G.STRICT + G.BOUNDARY + G.ORDER6 + G.DRIVER + G.FIXED_UPDATES)
 def test_engine_matches_reference_run(engine_lib, name):
     d = G.load(name)
     p = G.params(d)

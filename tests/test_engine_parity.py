@@ -162,17 +162,58 @@ def test_fixed_ghosts_keep_initial_values(engine_lib, integ):
         assert np.array_equal(got[f][ny - 2:, -2:], w[f][2:4, -2:])
 
 
-def test_fixed_with_ghost_updates_is_rejected(engine_lib):
-    """The reference's driver (every cell), 2D gravity and 2D background
-    energy coupling also update ghost cells, which fixed boundaries would then
-    keep: those combinations are refused instead of silently differing."""
-    w, pos, dx = ot_rect(20, 20, seed=2)
-    bt = (P.BC_FIXED, P.BC_PERIODIC)
-    for kw in (dict(driver=P.DRIVER_GAUSS, drv_amp=0.1, drv_x0=(1.0, 1.0, 0.0),
-                    drv_sigma=(0.5, 0.5, 0.0)), dict(g=(0.2, 0.0))):
-        with pytest.raises(Exception, match="fixed"):
-            engine_lib.Engine(params_for(w, dx, boundtype=bt, **kw), w, pos)
-    wb = with_background(w)
-    with pytest.raises(Exception, match="fixed"):
-        engine_lib.Engine(params_for(wb, dx, boundtype=bt), wb, pos)
+FIXED_UPDATE_CASES = [
+    # (boundary types, gravity, background fields, driver)
+    ((P.BC_FIXED, P.BC_PERIODIC), (0.2, -0.1), False, False),
+    ((P.BC_PERIODIC, P.BC_FIXED), (-0.15, 0.25), False, False),
+    ((P.BC_FIXED, P.BC_CONTCD4), (0.0, 0.0), True, False),
+    ((P.BC_CONTCD4, P.BC_FIXED), (0.1, 0.1), True, False),
+    ((P.BC_FIXED, P.BC_PERIODIC), (0.0, 0.0), False, True),
+    ((P.BC_FIXED, P.BC_FIXED), (0.2, -0.1), True, True),
+    ((P.BC_SYMM, P.BC_FIXED), (0.1, -0.2), True, True),
+]
 
+
+@pytest.mark.parametrize("integ", [P.INT_EULER, P.INT_RK4])
+@pytest.mark.parametrize("bt,g,bg,drv", FIXED_UPDATE_CASES)
+def test_parity_fixed_ghost_updates(engine_lib, oracle, bt, g, bg, drv, integ):
+    """2D fixed boundaries with gravity, background fields or the driver: the
+    reference's gravity and energy-coupling kernels also update the two low
+    ghost layers, its driver every ghost layer, and the fixed boundary keeps
+    those values (src/centdiff2.cu:587-872); the engine's fixed ghost layers
+    follow, ghost cells and CFL maxima included."""
+    w, pos, dx = ot_rect(30, 26, seed=11)
+    if bg:
+        w = with_background(w)
+    kw = dict(driver=P.DRIVER_GAUSS, drv_amp=0.05, drv_period=0.4, drv_x0=(0.8, 2.0),
+              drv_sigma=(1.5, 2.0)) if drv else {}
+    p = params_for(w, dx, integrator=integ, boundtype=bt, g=g, **kw)
+    got, (it, t, dt), cm, ref = run_both(engine_lib, oracle, w, pos, p, 6)
+    assert_parity(got, ref)
+    assert abs(dt - ref.dt) <= 1e-13 * abs(ref.dt)
+    # the fixed ghost layers did change
+    w0 = oracle.boundary(p, w)
+    ny, nx = w.shape[1:]
+    mask = np.zeros((ny, nx), bool)
+    if bt[0] == P.BC_FIXED:
+        mask[:, [0, 1, nx - 2, nx - 1]] = True
+    if bt[1] == P.BC_FIXED:
+        mask[[0, 1, ny - 2, ny - 1], :] = True
+    assert any(not np.array_equal(got[f][mask], w0[f][mask]) for f in range(6))
+
+
+def test_fixed_ghost_updates_refused_by_batches(engine_lib):
+    """Batches keep fixed ghost layers constant; runs whose fixed layers the
+    reference would update are refused with a clear error."""
+    w, pos, dx = ot_rect(20, 20, seed=2)
+    p = params_for(w, dx, integrator=P.INT_RK4, boundtype=(P.BC_FIXED, P.BC_PERIODIC), g=(0.2, 0.0))
+    with pytest.raises(engine_lib.SmaugError) as e:
+        engine_lib.Batch([p], [w], [pos])
+    assert "fixed ghost" in str(e.value)
+
+
+def test_fixed_ghost_updates_need_order4(engine_lib):
+    w, pos, dx = ot_rect(20, 20, seed=2)
+    p = params_for(w, dx, boundtype=(P.BC_FIXED, P.BC_PERIODIC), g=(0.2, 0.0), stencil_order=6)
+    with pytest.raises(engine_lib.SmaugError, match="4th-order"):
+        engine_lib.Engine(p, w, pos)

@@ -13,7 +13,7 @@ from tests.util import rel_l2
 TOL = 1e-13
 
 
-@pytest.mark.parametrize("name", G.STRICT + G.BOUNDARY + G.ORDER6 + G.DRIVER)
+@pytest.mark.parametrize("name", G.STRICT + G.BOUNDARY + G.ORDER6 + G.DRIVER + G.FIXED_UPDATES)
 def test_oracle_matches_reference_run(oracle, name):
     d = G.load(name)
     p = G.params(d)
