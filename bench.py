@@ -284,24 +284,36 @@ def ensemble_main(args):
     prec = 0 if args.precision == "fp64" else 1
     runs = make_ensemble(args.nruns, precision=prec)
     cells = sum(r[3] for r in runs)
-    warm = max(args.warmup, 8)
-    b = engine.Batch([r[0] for r in runs], [r[1] for r in runs], [r[2] for r in runs])
+    warm = max(args.warmup, 12)  # the first 10 steps time the (tile shape, launch) candidates
     stream = torch.cuda.Stream()
-    b.set_stream(stream.cuda_stream)
-    b.step(warm)            # the first 8 steps time the (tile shape, grid) candidates
-    torch.cuda.synchronize()
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
-    with ClockSampler(0) as clk:
-        ev0.record(stream)
-        b.step_async(args.steps)
-        ev1.record(stream)
+
+    def timed_batch(form):
+        b = engine.Batch([r[0] for r in runs], [r[1] for r in runs], [r[2] for r in runs])
+        b.set_stream(stream.cuda_stream)
+        b.pin_form(form)
+        b.step(warm)
         torch.cuda.synchronize()
-    b.sync()
-    ms = ev0.elapsed_time(ev1)
-    shape = b.launch_shape()
-    shape["tile"] = b.tile_shape()
-    b.close()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        with ClockSampler(0) as clk:
+            ev0.record(stream)
+            b.step_async(args.steps)
+            ev1.record(stream)
+            torch.cuda.synchronize()
+        b.sync()
+        shape = b.launch_shape()
+        shape["tile"] = b.tile_shape()
+        shape["persistent"] = b.persistent()
+        b.close()
+        return ev0.elapsed_time(ev1), shape, clk
+
+    ms, shape, clk = timed_batch(None)           # the autotuner's choice
+    forms = {}
+    for form in ("per-stage", "persistent"):     # each form alone, steady state
+        fms, fshape, _ = timed_batch(form)
+        forms[form] = {"value": cells * args.steps / (fms / 1e3) / 1e6, "unit": UNIT,
+                       "ms_per_step": fms / args.steps, "tile": fshape["tile"]["tile"],
+                       "grid": fshape["grid"]}
     # one by one: each run alone, its own engine and stream, same step counts
     ms_single = 0.0
     for p, w, pos, nc in runs:
@@ -337,6 +349,7 @@ def ensemble_main(args):
         "one_by_one": {"value": single, "unit": UNIT, "ms_per_step": ms_single / args.steps},
         "speedup_vs_one_by_one": value / single,
         "launch_shape": shape,
+        "forms": forms,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "alg_bytes_per_cell_step": mbytes,
                      "scheme_bytes_per_cell_step": scheme_bytes_per_cell_step(2, bool(prec)),

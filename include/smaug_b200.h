@@ -203,13 +203,16 @@ int smaug_destroy(smaug_handle_t h);
 /* ---- batched ensemble of independent 2D runs ----------------------------
  * No counterpart in the reference (one run per process there).  Runs of any
  * size, boundary types, background fields and driver advance together with
- * classical RK4: every stage of every run is one launch over the tile list of
- * all runs, and a cycle of 6 steps is captured once into a CUDA graph and
- * replayed.  All runs share one precision form.  The first 8 steps time 2
- * tile shapes (32x8, 16x16) x 4 launch shapes (1 and 2 blocks per SM, the
- * occupancy limit per SM, one block per tile) and keep the fastest; results
- * do not depend on either shape.  Each
- * run's results equal those of the same run stepped alone with smaug_step. */
+ * classical RK4 over the tile list of all runs, in one of two forms: one
+ * launch per stage, or one persistent launch for several steps whose blocks
+ * take tiles from a shared counter and meet at a grid barrier between stages.
+ * A cycle of 6 steps is captured once into a CUDA graph and replayed (24 stage
+ * launches, or one persistent launch).  All runs share one precision form.
+ * The first 10 steps time 2 tile shapes (32x8, 16x16) x 5 launch shapes (1 and
+ * 2 blocks per SM, the occupancy limit per SM, one block per tile, the
+ * persistent launch) and keep the fastest; results do not depend on either
+ * shape.  Each run's results equal those of the same run stepped alone with
+ * smaug_step. */
 typedef struct smaug_batch_s* smaug_batch_t;
 
 /* params[r], w[r], pos[r]: as smaug_create for run r (2D, integrator RK4) */
@@ -235,6 +238,12 @@ int smaug_batch_launch_shape(smaug_batch_t b, int32_t* grid, int32_t* candidates
 int smaug_batch_tile_shape(smaug_batch_t b, int32_t* tx, int32_t* ty, float* ms);
 /* Use only tile shape tx x ty (32x8 or 16x16); call before the first step. */
 int smaug_batch_pin_tile_shape(smaug_batch_t b, int32_t tx, int32_t ty);
+/* The persistent launch: *on = 1 when the tuner chose it; grid[2] its blocks
+   and ms[2] its step time per tile shape (32x8, 16x16; 0 when not timed). */
+int smaug_batch_persistent(smaug_batch_t b, int32_t* on, int32_t* grid, float* ms);
+/* Restrict the tuner to one form: -1 both (default), 0 per-stage launches,
+   1 the persistent launch; call before the first step. */
+int smaug_batch_pin_form(smaug_batch_t b, int32_t form);
 int smaug_batch_destroy(smaug_batch_t b);
 
 /* ---- adjoint of one RK4 step (2D, FP64, dt held fixed) -------------------

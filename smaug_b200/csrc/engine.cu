@@ -920,12 +920,15 @@ extern "C" int smaug_destroy(smaug_handle_t h) {
 // ===========================================================================
 // Batched ensemble of 2D runs
 // ===========================================================================
-// Independent runs advance together: each stage of every run is one launch of
-// stage2d_batch over the concatenated tile list of all runs, and a cycle of 6
-// RK4 steps (the period of the dt/t double buffers, 2, and of the CFL-maxima
-// ring, 3 slots advanced 4 times per step) is captured once into a CUDA graph
-// and replayed.  Each run keeps its own engine state (buffers, dt, time, CFL
-// maxima), so a run's results are those of the same run stepped alone.
+// Independent runs advance together over the concatenated tile list of all
+// runs, in one of two forms the autotuner chooses between: one launch of
+// stage2d_batch per stage, or one persistent launch of stage2d_batch_cycle
+// for several steps (its blocks meet at a grid barrier between stages).  A
+// cycle of 6 RK4 steps (the period of the dt/t double buffers, 2, and of the
+// CFL-maxima ring, 3 slots advanced 4 times per step) is captured once into a
+// CUDA graph and replayed: 24 stage launches, or one persistent launch.  Each
+// run keeps its own engine state (buffers, dt, time, CFL maxima), so a run's
+// results are those of the same run stepped alone.
 namespace smaug {
 
 constexpr int BATCH_CYCLE = 6;
@@ -934,14 +937,22 @@ constexpr int BATCH_CYCLE = 6;
 struct BatchShape {
   int tx, ty;
   cudaError_t (*launch)(int, bool, const KParams*, const KBufs*, const int4*, int, int, cudaStream_t);
+  cudaError_t (*launch_cycle)(bool, const KParams*, const KBufs*, const int4*, int, int, int, int, BatchSync*,
+                              int*, int, cudaStream_t);
   cudaError_t (*set_attributes)();
   int (*max_blocks_per_sm)(bool);
+  int (*cycle_max_blocks_per_sm)(bool);
 };
 constexpr int NSHAPES = 2;
 static const BatchShape kShapes[NSHAPES] = {
-    {32, 8, t32x8::launch_batch2d, t32x8::batch2d_set_attributes, t32x8::batch2d_max_blocks_per_sm},
-    {16, 16, t16x16::launch_batch2d, t16x16::batch2d_set_attributes, t16x16::batch2d_max_blocks_per_sm},
+    {32, 8, t32x8::launch_batch2d, t32x8::launch_batch2d_cycle, t32x8::batch2d_set_attributes,
+     t32x8::batch2d_max_blocks_per_sm, t32x8::batch2d_cycle_max_blocks_per_sm},
+    {16, 16, t16x16::launch_batch2d, t16x16::launch_batch2d_cycle, t16x16::batch2d_set_attributes,
+     t16x16::batch2d_max_blocks_per_sm, t16x16::batch2d_cycle_max_blocks_per_sm},
 };
+// candidates per tile shape: 4 grids of per-stage launches, then the
+// persistent launch
+constexpr int NCAND = 5;
 
 struct Batch {
   std::vector<Engine*> runs;
@@ -957,6 +968,12 @@ struct Batch {
   int grid_candidates[NSHAPES][4] = {};
   float grid_ms[NSHAPES][4] = {};
   int tuned = 0;            // (shape, grid) candidates timed so far
+  bool persistent = false;  // the chosen form: the persistent launch
+  int pin_form = -1;        // -1 tuned, 0 per-stage launches only, 1 persistent only
+  int cycle_grid[NSHAPES] = {};   // blocks of the persistent launch (all co-resident)
+  float cycle_ms[NSHAPES] = {};   // its step time per tile shape
+  BatchSync* d_sync = nullptr;    // its grid barrier and tile counters
+  int* d_err = nullptr;           // set when one of its barrier waits gave up
   long steps = 0;
   cudaGraphExec_t cycle = nullptr;
   cudaStream_t own_stream = nullptr;  // the batch's stream while a caller stream is set
@@ -968,6 +985,8 @@ static void free_batch(Batch* b) {
   if (b->cycle) cudaGraphExecDestroy(b->cycle);
   cudaFree(b->d_K);
   cudaFree(b->d_B);
+  cudaFree(b->d_sync);
+  cudaFree(b->d_err);
   for (int s = 0; s < NSHAPES; s++) cudaFree(b->d_tiles[s]);
   for (Engine* e : b->runs) free_engine(e);
   cudaStreamDestroy(b->own_stream ? b->own_stream : b->stream);
@@ -987,6 +1006,15 @@ static int batch_enqueue_step(Batch* b, long k, int shape, int grid) {
                                    b->d_B + (size_t)batch_variant(s, parity, ring) * nr, b->d_tiles[shape],
                                    b->ntiles[shape], grid, b->stream));
   }
+  return SMAUG_OK;
+}
+
+// nsteps (<= BATCH_MAX_STEPS) RK4 steps of every run from global step k in one
+// persistent launch with tile shape `shape`
+static int batch_enqueue_persistent(Batch* b, long k, int nsteps, int shape) {
+  CUDA_TRY(kShapes[shape].launch_cycle(b->mix, b->d_K, b->d_B, b->d_tiles[shape], b->ntiles[shape],
+                                       (int)b->runs.size(), (int)(k % BATCH_CYCLE), nsteps, b->d_sync,
+                                       b->d_err, b->cycle_grid[shape], b->stream));
   return SMAUG_OK;
 }
 
@@ -1082,7 +1110,13 @@ static int batch_create(int nruns, const smaug_params_t* const* params, const do
     gc[1] = 2 * nsm < nt ? 2 * nsm : nt;
     gc[2] = occ * nsm < nt ? occ * nsm : nt;
     gc[3] = nt;
+    // the persistent launch: every block resident at once
+    int occ_c = kShapes[sh].cycle_max_blocks_per_sm(b->mix);
+    b->cycle_grid[sh] = occ_c >= 1 ? (occ_c * nsm < nt ? occ_c * nsm : nt) : 0;
   }
+  B_TRY(cudaMalloc(&b->d_sync, sizeof(BatchSync)));
+  B_TRY(cudaMalloc(&b->d_err, sizeof(int)));
+  B_TRY(cudaMemset(b->d_err, 0, sizeof(int)));
 #undef B_TRY
   *out = b;
   return SMAUG_OK;
@@ -1107,28 +1141,38 @@ static int batch_tune(Batch* b, int* nsteps) {
   cudaEvent_t* ev = pair.ev;
   CUDA_TRY(cudaEventCreate(&ev[0]));
   CUDA_TRY(cudaEventCreate(&ev[1]));
-  for (int c = b->tuned; c < NSHAPES * 4 && *nsteps > 0; c++) {
-    const int sh = c / 4, g = c % 4;
+  auto wanted = [&](int sh, int g) {
+    if (b->pinned >= 0 && sh != b->pinned) return false;
+    if (g == NCAND - 1) return b->pin_form != 0 && b->cycle_grid[sh] > 0;
+    return b->pin_form != 1;
+  };
+  for (int c = b->tuned; c < NSHAPES * NCAND && *nsteps > 0; c++) {
+    const int sh = c / NCAND, g = c % NCAND;
     b->tuned = c + 1;
-    if (b->pinned >= 0 && sh != b->pinned) continue;
+    if (!wanted(sh, g)) continue;
     CUDA_TRY(cudaEventRecord(ev[0], b->stream));
-    int rc = batch_enqueue_step(b, b->steps, sh, b->grid_candidates[sh][g]);
+    int rc = g == NCAND - 1 ? batch_enqueue_persistent(b, b->steps, 1, sh)
+                            : batch_enqueue_step(b, b->steps, sh, b->grid_candidates[sh][g]);
     if (rc) return rc;
     CUDA_TRY(cudaEventRecord(ev[1], b->stream));
     CUDA_TRY(cudaEventSynchronize(ev[1]));
-    CUDA_TRY(cudaEventElapsedTime(&b->grid_ms[sh][g], ev[0], ev[1]));
+    CUDA_TRY(cudaEventElapsedTime(g == NCAND - 1 ? &b->cycle_ms[sh] : &b->grid_ms[sh][g], ev[0], ev[1]));
     batch_advance_bookkeeping(b, 1);
     (*nsteps)--;
   }
-  if (b->tuned == NSHAPES * 4) {
+  if (b->tuned == NSHAPES * NCAND) {
     int bs = -1, bg = 0;
-    for (int sh = 0; sh < NSHAPES; sh++) {
-      if (b->pinned >= 0 && sh != b->pinned) continue;
-      for (int g = 0; g < 4; g++)
-        if (bs < 0 || b->grid_ms[sh][g] < b->grid_ms[bs][bg]) bs = sh, bg = g;
-    }
+    float best = 0;
+    for (int sh = 0; sh < NSHAPES; sh++)
+      for (int g = 0; g < NCAND; g++) {
+        if (!wanted(sh, g)) continue;
+        const float ms = g == NCAND - 1 ? b->cycle_ms[sh] : b->grid_ms[sh][g];
+        if (bs < 0 || ms < best) bs = sh, bg = g, best = ms;
+      }
+    if (bs < 0) return set_error(SMAUG_E_CUDA, "no launch form of the batch could be timed");
     b->shape = bs;
-    b->grid = b->grid_candidates[bs][bg];
+    b->persistent = bg == NCAND - 1;
+    b->grid = b->persistent ? b->cycle_grid[bs] : b->grid_candidates[bs][bg];
   }
   return SMAUG_OK;
 }
@@ -1144,7 +1188,10 @@ static int batch_enqueue(Batch* b, int nsteps) {
         cudaGraph_t g = nullptr;
         CUDA_TRY(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
         int rc = SMAUG_OK;
-        for (int k = 0; k < BATCH_CYCLE && !rc; k++) rc = batch_enqueue_step(b, k, b->shape, b->grid);
+        if (b->persistent)
+          rc = batch_enqueue_persistent(b, 0, BATCH_CYCLE, b->shape);
+        else
+          for (int k = 0; k < BATCH_CYCLE && !rc; k++) rc = batch_enqueue_step(b, k, b->shape, b->grid);
         cudaError_t ce = cudaStreamEndCapture(b->stream, &g);
         if (rc || ce != cudaSuccess) {
           if (g) cudaGraphDestroy(g);
@@ -1159,7 +1206,8 @@ static int batch_enqueue(Batch* b, int nsteps) {
       batch_advance_bookkeeping(b, BATCH_CYCLE);
       nsteps -= BATCH_CYCLE;
     } else {
-      int rc = batch_enqueue_step(b, b->steps, b->shape, b->grid);
+      int rc = b->persistent ? batch_enqueue_persistent(b, b->steps, 1, b->shape)
+                             : batch_enqueue_step(b, b->steps, b->shape, b->grid);
       if (rc) return rc;
       batch_advance_bookkeeping(b, 1);
       nsteps--;
@@ -1170,6 +1218,9 @@ static int batch_enqueue(Batch* b, int nsteps) {
 
 static int batch_sync(Batch* b) {
   CUDA_TRY(cudaStreamSynchronize(b->stream));
+  int err = 0;
+  CUDA_TRY(cudaMemcpy(&err, b->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (err) return set_error(SMAUG_E_CUDA, "persistent batch launch: a grid-barrier wait timed out");
   for (Engine* e : b->runs) {
     int rc = sync_check(e);
     if (rc) return rc;
@@ -1266,6 +1317,33 @@ extern "C" int smaug_batch_tile_shape(smaug_batch_t h, int32_t* tx, int32_t* ty,
   if (ms)
     for (int sh = 0; sh < smaug::NSHAPES; sh++)
       for (int g = 0; g < 4; g++) ms[sh * 4 + g] = b->grid_ms[sh][g];
+  return SMAUG_OK;
+}
+
+extern "C" int smaug_batch_persistent(smaug_batch_t h, int32_t* on, int32_t* grid, float* ms) {
+  smaug::clear_error();
+  if (!h) return smaug::set_error(SMAUG_E_INVALID, "null handle");
+  Batch* b = HB(h);
+  if (on) *on = b->grid != 0 && b->persistent ? 1 : 0;
+  for (int sh = 0; sh < smaug::NSHAPES; sh++) {
+    if (grid) grid[sh] = b->cycle_grid[sh];
+    if (ms) ms[sh] = b->cycle_ms[sh];
+  }
+  return SMAUG_OK;
+}
+
+extern "C" int smaug_batch_pin_form(smaug_batch_t h, int32_t form) {
+  smaug::clear_error();
+  if (!h) return smaug::set_error(SMAUG_E_INVALID, "null handle");
+  Batch* b = HB(h);
+  if (b->tuned > 0 || b->grid != 0)
+    return smaug::set_error(SMAUG_E_INVALID, "the launch form is chosen at the first step: pin it before");
+  if (form < -1 || form > 1) return smaug::set_error(SMAUG_E_INVALID, "form must be -1, 0 or 1");
+  if (form == 1)
+    for (int sh = 0; sh < smaug::NSHAPES; sh++)
+      if (b->cycle_grid[sh] <= 0 && (b->pinned < 0 || b->pinned == sh))
+        return smaug::set_error(SMAUG_E_UNSUPPORTED, "no resident grid for the persistent launch");
+  b->pin_form = form;
   return SMAUG_OK;
 }
 

@@ -110,6 +110,22 @@ struct Form<true> {
 // ---------------------------------------------------------------------------
 // device helpers
 // ---------------------------------------------------------------------------
+// Loads of a stage's input.  Kernels that run one stage per launch read the
+// state through the read-only path (CG = false); a kernel that runs several
+// stages in one launch reads what other blocks wrote in an earlier stage of
+// the same launch, which only L2 holds coherently, so it loads with .cg
+// (CG = true).  ldin: arrays (read-only path by default), ldsc: scalars
+// (plain loads by default).
+template <bool CG, typename T>
+__device__ __forceinline__ T ldin(const T* p) {
+  if (CG) return __ldcg(p);
+  return __ldg(p);
+}
+template <bool CG, typename T>
+__device__ __forceinline__ T ldsc(const T* p) {
+  if (CG) return __ldcg(p);
+  return *p;
+}
 __device__ __forceinline__ double dmax0(double m, double v) { return (v > m) ? v : m; }
 template <typename T>
 __device__ __forceinline__ T hmax0(T m, T v) { return (v > m) ? v : m; }
@@ -261,11 +277,11 @@ __device__ __forceinline__ double dflux(const double* a, int l, int s, double rd
 __device__ __forceinline__ bool edge6(int a, int n) { return a == 2 || a == n - 3; }
 
 // base state of a field value (the RK4 base / the Euler input) in double
-template <bool MIX>
+template <bool MIX, bool CG = false>
 __device__ __forceinline__ double base_value(const KBufs& B, long idx) {
   if (MIX)
-    return (double)static_cast<const float*>(B.un)[idx] + (double)B.un_lo[idx];
-  return static_cast<const double*>(B.un)[idx];
+    return (double)ldsc<CG>(static_cast<const float*>(B.un) + idx) + (double)ldsc<CG>(B.un_lo + idx);
+  return ldsc<CG>(static_cast<const double*>(B.un) + idx);
 }
 
 // store of one stage result; a base state keeps a float high/low pair in the
@@ -303,6 +319,16 @@ cudaError_t stage3d_set_attributes();
 // the fixed ghost layers of a 2D stage, after the stage launch (stage2d.cu)
 cudaError_t launch_fixed_ghost2d(int mode, bool mix, const KParams& K, const KBufs& B, cudaStream_t st);
 
+// Device state of the persistent batch kernel (one launch runs several RK4
+// steps of every run): a grid barrier (arrival count, generation) and one
+// tile counter per stage; zeroed before every launch.
+constexpr int BATCH_MAX_STEPS = 6;
+struct BatchSync {
+  unsigned int count;
+  unsigned int gen;
+  int next[4 * BATCH_MAX_STEPS];
+};
+
 // batched 2D stages (batch_kernel.cuh), one instantiation per tile shape
 // (batch.cu: 32x8, batch16.cu: 16x16): Ks/Bs per run in device memory,
 // tiles = (run, tile x, tile y) work list of that shape, `grid` persistent
@@ -310,8 +336,13 @@ cudaError_t launch_fixed_ghost2d(int mode, bool mix, const KParams& K, const KBu
 #define SMAUG_BATCH_DECL                                                                        \
   cudaError_t launch_batch2d(int mode, bool mix, const KParams* Ks, const KBufs* Bs,           \
                              const int4* tiles, int ntiles, int grid, cudaStream_t st);         \
+  cudaError_t launch_batch2d_cycle(bool mix, const KParams* Ks, const KBufs* Bs,              \
+                                   const int4* tiles, int ntiles, int nruns, int k0,           \
+                                   int nsteps, BatchSync* sync, int* err, int grid,            \
+                                   cudaStream_t st);                                            \
   cudaError_t batch2d_set_attributes();                                                         \
-  int batch2d_max_blocks_per_sm(bool mix);
+  int batch2d_max_blocks_per_sm(bool mix);                                                      \
+  int batch2d_cycle_max_blocks_per_sm(bool mix);
 namespace t32x8 { SMAUG_BATCH_DECL }
 namespace t16x16 { SMAUG_BATCH_DECL }
 #undef SMAUG_BATCH_DECL

@@ -128,25 +128,26 @@ __device__ __forceinline__ double hq_at(const T2<BG, MIX>& T, int l) {
 }
 
 // the same q from global memory (stray pad source cell)
-template <typename ST, int KIND, int COMP>
+template <typename ST, int KIND, int COMP, bool CG = false>
 __device__ __forceinline__ double hq_global(const ST* u, const double* bg, long nc, long c) {
-  const double rho = u[0 * nc + c], rhob = bg[1 * nc + c];
+  auto ld = [&](long i) { return CG ? (double)__ldcg(u + i) : (double)u[i]; };
+  const double rho = ld(0 * nc + c), rhob = bg[1 * nc + c];
   if (KIND == 0) return rho;
   const double r = 1.0 / (rho + rhob);
   if (KIND == 1) {
-    const double m1 = u[1 * nc + c], m2 = u[2 * nc + c];
-    const double b1 = u[4 * nc + c], b2 = u[5 * nc + c];
-    return (double)u[3 * nc + c] - 0.5 * ((b1 * b1 + b2 * b2) + (m1 * m1 + m2 * m2) * r);
+    const double m1 = ld(1 * nc + c), m2 = ld(2 * nc + c);
+    const double b1 = ld(4 * nc + c), b2 = ld(5 * nc + c);
+    return ld(3 * nc + c) - 0.5 * ((b1 * b1 + b2 * b2) + (m1 * m1 + m2 * m2) * r);
   }
-  if (KIND == 2) return (double)u[(1 + COMP) * nc + c] * r;
-  return u[(4 + COMP) * nc + c];
+  if (KIND == 2) return ld((1 + COMP) * nc + c) * r;
+  return ld((4 + COMP) * nc + c);
 }
 
 // (A) q of one hyperdiffusion field on the whole staged region, with the
 // reference's pads: index -1 along an axis holds the copy of index 5
 // (bc_hyperdifl), index n the stray tmp6 store of hyperdifvisc1r_parallel
 // (source table B.padsrc).  The passes of both directions read it.
-template <bool BG, bool MIX, int KIND, int COMP>
+template <bool BG, bool MIX, int KIND, int COMP, bool CG = false>
 __device__ __forceinline__ void stage_q2(const T2<BG, MIX>& T, const KParams& P, const KBufs& B,
                                          int tid) {
   using HT = typename Form<MIX>::H;
@@ -171,14 +172,14 @@ __device__ __forceinline__ void stage_q2(const T2<BG, MIX>& T, const KParams& P,
         q = hq_at<BG, MIX, KIND, COMP>(T, r + 6);
       } else if (ci == n0) {
         const int src = B.padsrc[0][cj];
-        if (src >= 0) q = hq_global<ST, KIND, COMP>(static_cast<const ST*>(B.uin), B.bg, nc, src);
+        if (src >= 0) q = hq_global<ST, KIND, COMP, CG>(static_cast<const ST*>(B.uin), B.bg, nc, src);
       }
     } else if (inx) {
       if (cj == -1) {
         q = hq_at<BG, MIX, KIND, COMP>(T, r + 6 * RX);
       } else if (cj == n1) {
         const int src = B.padsrc[1][ci];
-        if (src >= 0) q = hq_global<ST, KIND, COMP>(static_cast<const ST*>(B.uin), B.bg, nc, src);
+        if (src >= 0) q = hq_global<ST, KIND, COMP, CG>(static_cast<const ST*>(B.uin), B.bg, nc, src);
       }
     }
     Q[r] = (HT)q;
@@ -200,7 +201,7 @@ __device__ __forceinline__ void stage_q2(const T2<BG, MIX>& T, const KParams& P,
 template <bool BG, bool MIX, int KIND, int COMP, int DIM>
 __device__ __forceinline__ void hyper_pass(const T2<BG, MIX>& T, const KParams& P, const KBufs& B,
                                            int tid, bool active, int lxo, int lyo, int gi, int gj,
-                                           double dt, double* out) {
+                                           double dt, const double* cin, double* out) {
   using HT = typename Form<MIX>::H;
   constexpr int SX = (DIM == 0), SY = (DIM == 1);
   constexpr int QFIELD = (KIND == 0) ? RHO : (KIND == 1) ? EN : (KIND == 2) ? M1 + COMP : B1 + COMP;
@@ -224,7 +225,7 @@ __device__ __forceinline__ void hyper_pass(const T2<BG, MIX>& T, const KParams& 
   constexpr int oxN = (DIM == 0) ? HALO : HALO - 1, oyN = (DIM == 0) ? HALO - 1 : HALO;
   auto ri = [&](int lx, int ly) { return (ly - oyR) * exR + (lx - oxR); };
   auto ni = [&](int lx, int ly) { return (ly - oyN) * exN + (lx - oxN); };
-  const HT coef = (HT)(B.cmax_in[DIM] * P.chyp[QFIELD]);
+  const HT coef = (HT)(cin[DIM] * P.chyp[QFIELD]);
 
   // (B) R = max D3(i-1..i+1) / max D1(i-2..i+2) from q(i-2..i+3)
   for (int r = tid; r < exR * eyR; r += NTHREADS) {
@@ -343,7 +344,7 @@ __device__ __forceinline__ void hyper_pass(const T2<BG, MIX>& T, const KParams& 
 
 // The stage for tile (bx, by) of one grid; the single-run kernel below and
 // the batched kernel (batch.cu) call it.
-template <int MODE, bool BG, bool MIX, bool O6 = false>
+template <int MODE, bool BG, bool MIX, bool O6 = false, bool CG = false>
 __device__ __forceinline__ void stage2d_body(const KParams& P, const KBufs& B, int bx, int by) {
   using ST = typename Form<MIX>::S;
   extern __shared__ double smem[];
@@ -379,7 +380,7 @@ __device__ __forceinline__ void stage2d_body(const KParams& P, const KBufs& B, i
     double rho = 0.0, rhob = 1.0;
 #pragma unroll
     for (int f = 0; f < 6; f++) {
-      const ST v = in ? __ldg(uin + f * nc + c) : (ST)0;
+      const ST v = in ? ldin<CG>(uin + f * nc + c) : (ST)0;
       T.S[f * RC + r] = v;
       if (f == 0) rho = v;
     }
@@ -416,18 +417,19 @@ __device__ __forceinline__ void stage2d_body(const KParams& P, const KBufs& B, i
   }
 
   // ---- dt of this step and stage time ----------------------------------
+  const double cin[2] = {ldsc<CG>(B.cmax_in), ldsc<CG>(B.cmax_in + 1)};
   double dt, tstage;
   if (B.stage == 0) {
-    dt = device_dt(P, B.cmax_in, *B.dt_prev, 2);
+    dt = device_dt(P, cin, ldsc<CG>(B.dt_prev), 2);
     if (bx == 0 && by == 0 && tid == 0) {
       *B.dt_new = dt;
-      *B.t_new = *B.t_prev + dt;
+      *B.t_new = ldsc<CG>(B.t_prev) + dt;
       B.cmax_clear[0] = B.cmax_clear[1] = B.cmax_clear[2] = 0ull;
     }
-    tstage = *B.t_prev;
+    tstage = ldsc<CG>(B.t_prev);
   } else {
-    dt = *B.dt_new;
-    tstage = *B.t_prev + (B.stage == 3 ? dt : 0.5 * dt);
+    dt = ldsc<CG>(B.dt_new);
+    tstage = ldsc<CG>(B.t_prev) + (B.stage == 3 ? dt : 0.5 * dt);
     if (bx == 0 && by == 0 && tid == 0)
       B.cmax_clear[0] = B.cmax_clear[1] = B.cmax_clear[2] = 0ull;
   }
@@ -444,7 +446,7 @@ __device__ __forceinline__ void stage2d_body(const KParams& P, const KBufs& B, i
     if (MODE != SMAUG_INT_EULER)
       out[f] = 0.0;
     else if (MIX)
-      out[f] = active ? base_value<MIX>(B, f * nc + co) : 0.0;
+      out[f] = active ? base_value<MIX, CG>(B, f * nc + co) : 0.0;
     else
       out[f] = T.v(f, lo);
   }
@@ -517,8 +519,8 @@ __device__ __forceinline__ void stage2d_body(const KParams& P, const KBufs& B, i
 
   // ---- hyperdiffusion, in the driver's order -------------------------------
   if (P.hyperdif == 1) {
-#define HP(K, C, D) hyper_pass<BG, MIX, K, C, D>(T, P, B, tid, active, lxo, lyo, gi, gj, dt, out)
-#define SQ(K, C) stage_q2<BG, MIX, K, C>(T, P, B, tid)
+#define HP(K, C, D) hyper_pass<BG, MIX, K, C, D>(T, P, B, tid, active, lxo, lyo, gi, gj, dt, cin, out)
+#define SQ(K, C) stage_q2<BG, MIX, K, C, CG>(T, P, B, tid)
     SQ(0, 0); HP(0, 0, 0); HP(0, 0, 1);
     SQ(1, 0); HP(1, 0, 0); HP(1, 0, 1);
     SQ(2, 0); HP(2, 0, 0); HP(2, 0, 1);
@@ -561,14 +563,14 @@ __device__ __forceinline__ void stage2d_body(const KParams& P, const KBufs& B, i
       for (int f = 0; f < 6; f++) {
         const double dl = out[f];
         if (B.stage == 0) {
-          const double u = MIX ? base_value<MIX>(B, f * nc + co) : T.v(f, lo);
+          const double u = MIX ? base_value<MIX, CG>(B, f * nc + co) : T.v(f, lo);
           B.acc[f * nc + co] = u + wgt * dl;
           res[f] = u + cst * dl;
         } else if (B.stage < 3) {
-          B.acc[f * nc + co] = B.acc[f * nc + co] + wgt * dl;
-          res[f] = base_value<MIX>(B, f * nc + co) + cst * dl;
+          B.acc[f * nc + co] = ldsc<CG>(B.acc + f * nc + co) + wgt * dl;
+          res[f] = base_value<MIX, CG>(B, f * nc + co) + cst * dl;
         } else {
-          res[f] = B.acc[f * nc + co] + wgt * dl;
+          res[f] = ldsc<CG>(B.acc + f * nc + co) + wgt * dl;
         }
       }
     }

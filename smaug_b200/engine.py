@@ -27,6 +27,7 @@ EXPORTS = [
     "smaug_adj_tape_reserve", "smaug_adj_forward_tape", "smaug_adj_backward_tape",
     "smaug_adj_destroy", "smaug_write_out_async", "smaug_wait_writes",
     "smaug_adj_backward_tape_range", "smaug_batch_tile_shape", "smaug_batch_pin_tile_shape",
+    "smaug_batch_persistent", "smaug_batch_pin_form",
 ]
 
 ERRORS = {1: "invalid", 2: "cuda", 3: "nomem", 4: "io", 5: "format", 6: "unsupported",
@@ -89,6 +90,10 @@ def lib():
         L.smaug_batch_tile_shape.argtypes = [vp, ctypes.POINTER(ctypes.c_int32),
                                              ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_float)]
         L.smaug_batch_pin_tile_shape.argtypes = [vp, ctypes.c_int32, ctypes.c_int32]
+        L.smaug_batch_persistent.argtypes = [vp, ctypes.POINTER(ctypes.c_int32),
+                                             ctypes.POINTER(ctypes.c_int32),
+                                             ctypes.POINTER(ctypes.c_float)]
+        L.smaug_batch_pin_form.argtypes = [vp, ctypes.c_int32]
         L.smaug_batch_launch_shape.argtypes = [vp, ctypes.POINTER(ctypes.c_int32),
                                                ctypes.POINTER(ctypes.c_int32),
                                                ctypes.POINTER(ctypes.c_float)]
@@ -320,6 +325,24 @@ class Batch:
     def pin_tile_shape(self, tx, ty):
         """Use only the tile shape tx x ty (32x8 or 16x16); before the first step."""
         _check(lib().smaug_batch_pin_tile_shape(self.h, int(tx), int(ty)))
+        return self
+
+    def persistent(self):
+        """Whether the tuner chose the persistent launch, and per tile shape
+        (32x8, 16x16) its resident grid and step time."""
+        on = ctypes.c_int32(0)
+        grid = (ctypes.c_int32 * 2)()
+        ms = (ctypes.c_float * 2)()
+        _check(lib().smaug_batch_persistent(self.h, ctypes.byref(on), grid, ms))
+        return {"on": bool(on.value), "grid": {"32x8": int(grid[0]), "16x16": int(grid[1])},
+                "ms": {"32x8": float(ms[0]), "16x16": float(ms[1])}}
+
+    def pin_form(self, form):
+        """Restrict the tuner: "persistent" (one launch for several steps),
+        "per-stage" (one launch per stage) or None (both); before the first
+        step."""
+        code = {None: -1, "per-stage": 0, "persistent": 1}[form]
+        _check(lib().smaug_batch_pin_form(self.h, code))
         return self
 
     def close(self):

@@ -43,26 +43,39 @@ def ensemble(precision):
     return runs
 
 
+@pytest.mark.parametrize("form", [None, "per-stage", "persistent"])
 @pytest.mark.parametrize("pin", [None, (32, 8), (16, 16)])
 @pytest.mark.parametrize("precision,tol", [(P.PREC_FP64, 1e-12), (P.PREC_MIXED, 1e-6)])
-def test_batch_matches_single_runs(engine_lib, precision, tol, pin):
+def test_batch_matches_single_runs(engine_lib, precision, tol, pin, form):
     """Every run of a batch against the same run stepped alone, with the tile
     shape chosen by the autotuner or pinned to each built shape (the
-    single-run kernel uses 32x8 tiles)."""
+    single-run kernel uses 32x8 tiles), and the launch form chosen by the
+    autotuner or pinned to per-stage launches or to the persistent launch
+    (several steps per launch, a grid barrier between stages)."""
     runs = ensemble(precision)
     b = engine_lib.Batch([r[0] for r in runs], [r[1] for r in runs], [r[2] for r in runs])
     if pin:
         b.pin_tile_shape(*pin)
-    nfirst = 20  # 8 (4 pinned) tuning steps, single steps, a 6-step graph cycle from step 12
+    b.pin_form(form)
+    # up to 10 tuning steps, single steps, a 6-step graph cycle from step 12,
+    # single steps
+    nfirst = 20
     b.step(nfirst)
     shape = b.launch_shape()
-    assert shape["grid"] in shape["candidates"]
+    pers = b.persistent()
+    assert pers["on"] == (form == "persistent") or form is None
+    if pers["on"]:
+        tile = b.tile_shape()["tile"]
+        assert shape["grid"] == pers["grid"]["%dx%d" % tile] > 0
+    else:
+        assert shape["grid"] in shape["candidates"]
     tile = b.tile_shape()
     assert tile["tile"] in ((32, 8), (16, 16))
     if pin:
         assert tile["tile"] == pin
-    else:
+    elif form is None:
         assert all(v > 0 for v in tile["ms"]["32x8"] + tile["ms"]["16x16"])
+        assert all(v > 0 for v in pers["ms"].values())
     for i, (p, w, pos) in enumerate(runs):
         e = engine_lib.Engine(p, w, pos)
         e.step(nfirst)
@@ -113,5 +126,8 @@ def test_batch_pin_tile_shape_rejects(engine_lib):
     b.step(1)
     with pytest.raises(engine_lib.SmaugError) as e:
         b.pin_tile_shape(16, 16)
+    assert e.value.code == 1
+    with pytest.raises(engine_lib.SmaugError) as e:
+        b.pin_form("persistent")
     assert e.value.code == 1
     b.close()
