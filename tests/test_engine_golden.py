@@ -56,17 +56,24 @@ def test_engine_first_step_outside_race_column(engine_lib, name):
 
 @pytest.mark.parametrize("name", G.RACE)
 def test_engine_200_steps_against_oracle(engine_lib, oracle, name):
-    """The engine and the oracle share the deterministic pad model; over 200
-    steps of the flow their rounding differences (~1e-16 per operation, sums
-    ordered differently) grow to ~1e-10, far below the reference's own
-    run-to-run spread (~3e-4) and below the stated 1e-8."""
+    """The engine and the oracle share the deterministic pad model; their
+    rounding differences (~1e-16 per operation, sums ordered differently)
+    grow with the chaotic flow.  Observed maxima over the six fields on a
+    B200: 4.7e-16 after 10 steps, 1.2e-14 after 50, 4.3e-13 after 100,
+    2.1e-12 after 150, 3.0e-11 after 200 -- far below the reference's own
+    run-to-run spread (2.8e-4 after 200 steps).  Bounds: 1e-12 after 50
+    steps, 3e-10 (ten times the observed value) after 200."""
     d = G.load(name)
     p = G.params(d)
     e = engine_lib.Engine(p, d["w0full"], d["pos"])
-    e.step(200)
-    got = e.state()
+    run = oracle.OracleRun(p, d["w0full"], d["pos"])
+    done = 0
+    for k, bound in ((50, 1e-12), (200, 3e-10)):
+        e.step(k - done)
+        run.advance(k - done)
+        done = k
+        got = e.state()
+        errs = [rel_l2(got[f], run.w[f]) for f in range(6)]
+        assert max(errs) <= bound, (k, errs)
     e.close()
-    ref = oracle.OracleRun(p, d["w0full"], d["pos"]).advance(200)
-    errs = [rel_l2(got[f], ref.w[f]) for f in range(6)]
-    assert max(errs) <= 1e-8, errs
 
