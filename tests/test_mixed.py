@@ -128,3 +128,19 @@ def test_mixed_roundtrip_and_determinism(engine_lib):
         assert rel_l2(s10b[f], s10[f]) <= 1e-12
     a.close()
     b.close()
+
+
+@pytest.mark.parametrize("integ", [P.INT_RK4, P.INT_EULER])
+def test_mixed_fixed_ghost_updates(engine_lib, oracle, integ):
+    """2D fixed boundaries with gravity, background fields and the driver:
+    the mixed form's fixed ghost layers (fixed_ghost2d_kernel with float
+    storage) follow the FP64 oracle within the 1e-5 bar, ghost cells
+    included."""
+    w, pos, dx = ot_rect(30, 26, seed=11)
+    w = with_background(w)
+    p = params_for(w, dx, integrator=integ, precision=P.PREC_MIXED,
+                   boundtype=(P.BC_FIXED, P.BC_FIXED), g=(0.2, -0.1), driver=P.DRIVER_GAUSS,
+                   drv_amp=0.05, drv_period=0.4, drv_x0=(0.8, 2.0), drv_sigma=(1.5, 2.0))
+    errs, _, ref = errors(engine_lib, oracle, w, pos, p, 10, 6)
+    assert max(errs) <= TOL, errs
+    assert max(errs) > 1e-12, errs
