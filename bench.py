@@ -404,16 +404,20 @@ def adjoint_main(args):
     rng = np.random.default_rng(12)
     shift = torch.tensor(1.0 + 0.05 * rng.standard_normal(3), dtype=torch.float64)
     line = None
-    for obs_z in [args.obs_z] + ([0.4e6] if abs(args.obs_z - 0.4e6) > 1.0 else []):
+    # the headline row is 0.4 Mm; the configured 3 Mm row is reported beside it
+    # and labelled: nothing the driver excites reaches it within 400 steps
+    for obs_z in [args.obs_z] + ([3.0e6] if abs(args.obs_z - 3.0e6) > 1.0 else []):
         res = _adjoint_case(args, sa, q, p, u0, pos, rhob, theta0, shift, obs_z, nsteps,
                             rollout, rollout_autograd)
         if line is None:
             line = res
         else:
-            line["observation_row_0p4Mm"] = {k: res[k] for k in (
-                "value", "loss", "grad", "fd", "fd_rel_err", "forward_ms", "forward_backward_ms",
-                "full_tape")}
-            line["observation_row_0p4Mm"]["config_observed_row_z_m"] = res["config"]["observed_row_z_m"]
+            sub = {k: res[k] for k in ("value", "loss", "grad", "forward_ms", "forward_backward_ms")}
+            sub["observed_row_z_m"] = res["config"]["observed_row_z_m"]
+            if res["loss"] == 0.0:
+                sub["degenerate"] = ("no signal reaches the row within the rollout: loss and gradient "
+                                     "are exactly 0 and every adjoint tile returns at its first barrier")
+            line["configured_row_3Mm"] = sub
     sa.close()
     print(json.dumps(line), flush=True)
 
@@ -482,17 +486,26 @@ def _adjoint_case(args, sa, q, p, u0, pos, rhob, theta0, shift, obs_z, nsteps, r
         return th.grad.clone()
 
     grad_t, ms_fb_t = timed(fwd_bwd_full_tape)
-    fd = []
-    for k in range(3):
-        h = 1e-4 * float(theta0[k])
-        vals = []
-        for sgn in (1, -1):
-            th = theta0.clone()
-            th[k] += sgn * h
-            with torch.no_grad():
-                vals.append(float(rollout(sa, th, u0, nsteps, loss_fn, checkpoint_every=20)))
-        fd.append((vals[0] - vals[1]) / (2 * h))
-    rel = [abs(float(grad[k]) - fd[k]) / max(abs(fd[k]), 1e-300) for k in range(3)]
+    def central_fd(hrel):
+        out = []
+        for k in range(3):
+            h = hrel * float(theta0[k])
+            vals = []
+            for sgn in (1, -1):
+                th = theta0.clone()
+                th[k] += sgn * h
+                with torch.no_grad():
+                    vals.append(float(rollout(sa, th, u0, nsteps, loss_fn, checkpoint_every=20)))
+            out.append((vals[0] - vals[1]) / (2 * h))
+        return out
+
+    def rel_err(fd):
+        return [abs(float(grad[k]) - fd[k]) / max(abs(fd[k]), 1e-300) for k in range(3)]
+
+    fd = central_fd(1e-4)          # the configured step
+    rel = rel_err(fd)
+    fd6 = central_fd(1e-6)         # closer to the limit (truncation error ~h^2)
+    rel6 = rel_err(fd6)
     cells = p.interior_cells()
     line = {
         "metric": "adjoint cost / forward cost (loss gradient over a 400-step RK4 rollout)",
@@ -505,6 +518,7 @@ def _adjoint_case(args, sa, q, p, u0, pos, rhob, theta0, shift, obs_z, nsteps, r
         "forward_ms": ms_fwd, "forward_backward_ms": ms_fb,
         "forward_mcell_updates_per_s": cells * nsteps / (ms_fwd / 1e3) / 1e6,
         "loss": float(L0), "grad": [float(g) for g in grad], "fd": fd, "fd_rel_err": rel,
+        "fd_h": 1e-4, "fd_h1e-6": {"fd": fd6, "fd_rel_err": rel6},
         "composed_checkpoint_autograd": {
             "value": ms_fb_c / ms_fwd, "forward_backward_ms": ms_fb_c,
             "grad": [float(g) for g in grad_c],
@@ -755,8 +769,9 @@ def main():
     ap.add_argument("--workload", default="ot", choices=["ot", "tube", "ensemble", "adjoint", "snapshots",
                                                         "accuracy"])
     ap.add_argument("--adj-steps", type=int, default=400)
-    ap.add_argument("--obs-z", type=float, default=3.0e6,
-                    help="height of the observed v_z row for --workload adjoint [m]")
+    ap.add_argument("--obs-z", type=float, default=0.4e6,
+                    help="height of the observed v_z row for --workload adjoint [m] (the "
+                         "configured 3 Mm row is reported beside it)")
     ap.add_argument("--nruns", type=int, default=64)
     ap.add_argument("--precision", default=None, choices=["fp64", "mixed"],
                     help="default: fp64 (ot, tube; mixed reported beside it), mixed (ensemble)")
