@@ -276,9 +276,10 @@ def make_ensemble(nruns=64, seed=5, precision=1):
 
 
 def ensemble_main(args):
-    """--workload ensemble: 64 uneven runs in one batch (one launch per stage
-    for all runs, 6-step CUDA graph cycles, autotuned tile and launch shape) against
-    the same runs stepped one by one through their own engines."""
+    """--workload ensemble: 64 uneven runs in one batch (per-stage or persistent
+    launches for all runs, 6-step CUDA graph cycles, autotuned tile shape and
+    launch form) against the same runs stepped one by one through their own
+    engines; each launch form is also timed alone (`forms`)."""
     import torch
     from smaug_b200 import engine
     prec = 0 if args.precision == "fp64" else 1

@@ -255,8 +255,9 @@ class Engine:
 
 class Batch:
     """An ensemble of independent 2D runs advanced together (RK4): one launch
-    per stage for all runs, a 6-step cycle replayed from a CUDA graph; the
-    first 8 steps choose the tile and launch shape by timing."""
+    per stage for all runs or one persistent launch for several steps, a
+    6-step cycle replayed from a CUDA graph; the first 10 steps choose the
+    tile shape and the launch shape or form by timing."""
 
     def __init__(self, params_list, w_list, pos_list):
         n = len(params_list)
