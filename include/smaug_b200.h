@@ -177,6 +177,19 @@ int smaug_get_time(smaug_handle_t h, int64_t* it, double* t, double* dt);
    src/computedervfields.cu:1864-2050). */
 int smaug_get_cmax(smaug_handle_t h, double* cmax);
 
+/* How the 2D stage kernel stages its tiles in shared memory: *tma = 0
+   per-thread loads, 1 bulk tensor copies (TMA) in a persistent grid whose
+   blocks copy their next tile during the current one's stores, 2 bulk
+   tensor copies with one block per tile; *available = 1 when the grid
+   admits the copies (2D, rows a multiple of 16 bytes in the storage type,
+   4th-order stencil).  Either pointer may be null.  No reference
+   counterpart: the reference stages no tiles. */
+int smaug_staging(smaug_handle_t h, int32_t* tma, int32_t* available);
+/* Select the staging of subsequent launches (0, 1 or 2 as above); the
+   results are bitwise identical.  SMAUG_E_UNSUPPORTED when 1 or 2 is asked
+   for and not available. */
+int smaug_set_staging(smaug_handle_t h, int32_t tma);
+
 /* Write the current state as a reference .out file (src/readwrite.c:160-366).
    `it` and `t` go to the header; name is the 79-byte run name. */
 int smaug_write_out(smaug_handle_t h, const char* path, const char* name,

@@ -17,7 +17,7 @@ ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libsmaug_b200.so")
 OBJDIR = os.path.join(HERE, "_build")
 CSRC = os.path.join(HERE, "csrc")
-SRCS = [os.path.join(CSRC, f) for f in ("engine.cu", "stage2d.cu", "stage3d.cu", "batch.cu", "batch16.cu",
+SRCS = [os.path.join(CSRC, f) for f in ("engine.cu", "stage2d.cu", "stage2d_tma.cu", "stage3d.cu", "batch.cu", "batch16.cu",
                                          "adjoint.cu", "host_io.cpp")]
 HEADERS = [os.path.join(CSRC, f) for f in sorted(os.listdir(CSRC)) if f.endswith((".h", ".cuh"))] + [
     os.path.join(ROOT, "include", "smaug_b200.h")]

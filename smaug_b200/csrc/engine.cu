@@ -181,6 +181,10 @@ struct Engine {
   int64_t it = 0;
   int device = 0;
   bool ghost_upd = false;                // 2D fixed ghost layers updated every stage
+  bool tma_ok = false;                   // 2D: tensor maps of every stage input exist
+  int tma = 0;                           // 2D staging: 0 per-thread loads, 1 bulk tensor copies
+                                         // (persistent grid), 2 bulk tensor copies (a block per tile)
+  TmaMap tm_u[3], tm_h[4], tm_bg;        // tensor maps of d_u / d_h / d_bg
   cudaStream_t own_stream = nullptr;     // created by the engine
   Snapshot snap[2];                      // asynchronous .out writes, used in turn
   int snap_next = 0;
@@ -448,9 +452,31 @@ static int create(const smaug_params_t* p, const double* w, const double* pos, E
   E_TRY(cudaMemset(e->d_flags, 0, sizeof(int)));
   E_TRY(stage2d_set_attributes());
   E_TRY(stage3d_set_attributes());
+  // 2D: tensor maps for the bulk tensor staging when the grid admits it
+  // (selected by smaug_set_staging; per-thread loads by default)
+  if (e->nd == 2 && stage2d_tma_supported(e->K, e->mix)) {
+    E_TRY(stage2d_tma_set_attributes());
+    bool ok = true;
+    for (int i = 0; i < 3 && ok; i++)
+      if (e->d_u[i]) ok = stage2d_tma_encode(&e->tm_u[i], e->d_u[i], false, e->K, e->nevo, e->nevo) == 0;
+    for (int i = 0; i < 4 && ok; i++)
+      if (e->d_h[i]) ok = stage2d_tma_encode(&e->tm_h[i], e->d_h[i], true, e->K, e->nevo, e->nevo) == 0;
+    if (ok) ok = stage2d_tma_encode(&e->tm_bg, e->d_bg, false, e->K, e->nbg, e->K.has_bg ? 4 : 1) == 0;
+    e->tma_ok = ok;
+    e->tma = 0;
+  }
 #undef E_TRY
   *out = e;
   return SMAUG_OK;
+}
+
+// tensor map of an engine buffer that is a stage input (null if none)
+static const TmaMap* tma_map_of(const Engine* e, const void* uin) {
+  for (int i = 0; i < 3; i++)
+    if (e->d_u[i] && uin == e->d_u[i]) return &e->tm_u[i];
+  for (int i = 0; i < 4; i++)
+    if (e->d_h[i] && uin == e->d_h[i]) return &e->tm_h[i];
+  return nullptr;
 }
 
 // FP64 state of the host interface <-> float high/low pair of the mixed form
@@ -590,7 +616,11 @@ static int launch_stage(Engine* e, int mode, int stage, const void* uin, const v
   if (e->nd == 3) {
     CUDA_TRY(launch_stage3d_any(mode, e->mix, K, B, e->stream));
   } else {
-    CUDA_TRY(launch_stage2d_any(mode, e->mix, K, B, e->stream));
+    const TmaMap* ms = e->tma ? tma_map_of(e, uin) : nullptr;
+    if (ms)
+      CUDA_TRY(launch_stage2d_tma(mode, e->mix, K, B, *ms, e->tm_bg, e->tma == 1, e->stream));
+    else
+      CUDA_TRY(launch_stage2d_any(mode, e->mix, K, B, e->stream));
     if (e->ghost_upd) CUDA_TRY(launch_fixed_ghost2d(mode, e->mix, K, B, e->stream));
   }
   e->stage_count++;
@@ -625,6 +655,11 @@ static int sync_check(Engine* e) {
   CUDA_TRY(cudaStreamSynchronize(e->stream));
   int flags = 0;
   CUDA_TRY(cudaMemcpy(&flags, e->d_flags, sizeof(int), cudaMemcpyDeviceToHost));
+  if (flags & FLAG_TMA_TIMEOUT) {
+    CUDA_TRY(cudaMemset(e->d_flags, 0, sizeof(int)));
+    return set_error(SMAUG_E_CUDA, "a bulk tensor copy of a stage tile did not complete in time (by step %lld)",
+                     (long long)e->it);
+  }
   if (flags & 1) {
     CUDA_TRY(cudaMemset(e->d_flags, 0, sizeof(int)));
     return set_error(SMAUG_E_NONFINITE, "non-finite value in the evolved state by step %lld",
@@ -839,6 +874,28 @@ extern "C" int smaug_get_cmax(smaug_handle_t h, double* cmax) {
   double c[3];
   CUDA_TRY(cudaMemcpy(c, e->d_cmax + 3 * (e->stage_count % 3), sizeof(c), cudaMemcpyDeviceToHost));
   for (int d = 0; d < e->nd; d++) cmax[d] = c[d];
+  return SMAUG_OK;
+}
+
+extern "C" int smaug_staging(smaug_handle_t h, int32_t* tma, int32_t* available) {
+  smaug::clear_error();
+  if (!h) return smaug::set_error(SMAUG_E_INVALID, "null handle");
+  Engine* e = H(h);
+  if (tma) *tma = e->tma;
+  if (available) *available = e->tma_ok ? 1 : 0;
+  return SMAUG_OK;
+}
+
+extern "C" int smaug_set_staging(smaug_handle_t h, int32_t tma) {
+  smaug::clear_error();
+  if (!h) return smaug::set_error(SMAUG_E_INVALID, "null handle");
+  Engine* e = H(h);
+  if (tma < 0 || tma > 2) return smaug::set_error(SMAUG_E_INVALID, "staging %d not in {0, 1, 2}", tma);
+  if (tma && !e->tma_ok)
+    return smaug::set_error(SMAUG_E_UNSUPPORTED,
+                            "bulk tensor staging needs a 2D grid whose rows are a multiple of 16 bytes "
+                            "in the storage type and the 4th-order stencil");
+  e->tma = tma;
   return SMAUG_OK;
 }
 

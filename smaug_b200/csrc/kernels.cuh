@@ -32,6 +32,7 @@ constexpr int RX = TX + 2 * HALO;  // staged region
 constexpr int RY = TY + 2 * HALO;
 constexpr int RC = RX * RY;
 constexpr int NTHREADS = TX * TY;
+constexpr int XORG = 2;            // x index of the first cell of tile column 0
 
 // 2D field ids (include/iotypes.h:209-216)
 enum { RHO = 0, M1 = 1, M2 = 2, EN = 3, B1 = 4, B2 = 5, EB = 6, RHOB = 7, BB1 = 8, BB2 = 9 };
@@ -126,6 +127,73 @@ __device__ __forceinline__ T ldsc(const T* p) {
   if (CG) return __ldcg(p);
   return *p;
 }
+// ---------------------------------------------------------------------------
+// bulk tensor copies (TMA) of a staged region into shared memory, completed
+// on an mbarrier (the TMA-staged 2D kernel, stage2d_tma.cu)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+  // the initialised barrier becomes visible to the copy engine
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+// orders the block's earlier shared-memory accesses (made visible to this
+// thread by a barrier) before the async copies this thread issues next
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+// box of a 3D tensor map ([z][y][x], x fastest) at (x, y, z) into shared
+// memory; x * element size must be a multiple of 16 bytes
+__device__ __forceinline__ void tma_load_3d(void* dst, const void* map, int x, int y, int z,
+                                            unsigned long long* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, "
+      "%4}], [%5];" ::"r"(smem_u32(dst)),
+      "l"(map), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+      : "memory");
+}
+// Wait until the barrier's phase of parity `parity` has completed; false
+// when it has not after limit_ns nanoseconds of the global timer.
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity, unsigned long long limit_ns) {
+  const unsigned a = smem_u32(bar);
+  unsigned long long t0 = 0;
+  for (unsigned i = 0;; i++) {
+    unsigned done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if ((i & 63) == 0) {
+      unsigned long long now;
+      asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
+      if (i == 0)
+        t0 = now;
+      else if (now - t0 > limit_ns)
+        return false;
+    }
+  }
+}
+constexpr unsigned long long TMA_WAIT_NS = 2000000000ull;  // 2 s
+constexpr int FLAG_TMA_TIMEOUT = 2;                         // KBufs::flags bit
+
+// the bulk-tensor staging of one tile of the TMA-staged 2D kernel
+struct TmaTile {
+  const void* ms;           // tensor map of the stage input, [field][y][x]
+  const void* mg;           // tensor map of the background fields, [field][y][x]
+  unsigned long long* bar;  // the block's mbarrier
+  unsigned parity;          // phase parity of this tile's copy
+  bool issue_self;          // the block's first tile: issue its own copy
+  int nbx, nby;             // the block's next tile (nbx < 0: none)
+};
+
 __device__ __forceinline__ double dmax0(double m, double v) { return (v > m) ? v : m; }
 template <typename T>
 __device__ __forceinline__ T hmax0(T m, T v) { return (v > m) ? v : m; }
@@ -318,6 +386,24 @@ cudaError_t stage2d_set_attributes();
 cudaError_t stage3d_set_attributes();
 // the fixed ghost layers of a 2D stage, after the stage launch (stage2d.cu)
 cudaError_t launch_fixed_ghost2d(int mode, bool mix, const KParams& K, const KBufs& B, cudaStream_t st);
+
+// TMA-staged 2D stage (stage2d_tma.cu).  TmaMap holds an encoded
+// CUtensorMap (128 bytes, 64-byte aligned).
+struct alignas(64) TmaMap {
+  unsigned char bytes[128];
+};
+// whether the grid admits bulk tensor staging (row pitch a multiple of 16
+// bytes in the storage type, no 6th-order stencil)
+bool stage2d_tma_supported(const KParams& K, bool mix);
+// tensor map of nfield [n1][n0] arrays at base (the stage input: nfield = 6,
+// box of all 6; the background fields: box of 4 from field 0 with bg, of
+// field 1 alone without); 0 on success
+int stage2d_tma_encode(TmaMap* m, const void* base, bool f32, const KParams& K, int nfield, int box_fields);
+// persistent: one block per resident slot, each staging its next tile
+// during the current one; else one block per tile
+cudaError_t launch_stage2d_tma(int mode, bool mix, const KParams& K, const KBufs& B, const TmaMap& ms,
+                               const TmaMap& mg, bool persistent, cudaStream_t st);
+cudaError_t stage2d_tma_set_attributes();
 
 // Device state of the persistent batch kernel (one launch runs several RK4
 // steps of every run): a grid barrier (arrival count, generation) and one

@@ -342,14 +342,38 @@ __device__ __forceinline__ void hyper_pass(const T2<BG, MIX>& T, const KParams& 
   __syncthreads();
 }
 
-// The stage for tile (bx, by) of one grid; the single-run kernel below and
-// the batched kernel (batch.cu) call it.
-template <int MODE, bool BG, bool MIX, bool O6 = false, bool CG = false>
-__device__ __forceinline__ void stage2d_body(const KParams& P, const KBufs& B, int bx, int by) {
+// Bulk tensor copy of the staged state of tile (bx, by) -- the 6 fields in
+// the storage type into T.S, and the 4 background fields into T.G (with
+// background fields) or rho_b alone into T.R (without) -- completing on
+// tt.bar.  Cells outside the grid read 0.  The region starts at column
+// x0 - HALO = XORG - HALO + bx TX, which the TMA-staged kernel's tile origin
+// makes a multiple of 32 cells (the copy's x offset must be 16-byte aligned).
+template <bool BG, bool MIX>
+__device__ __forceinline__ void tma_stage_issue(const T2<BG, MIX>& T, const TmaTile& tt, int bx, int by) {
+  using ST = typename Form<MIX>::S;
+  constexpr unsigned bytes = 6 * RC * sizeof(ST) + (BG ? 4 : 1) * RC * sizeof(double);
+  const int x = XORG - HALO + bx * TX, y = 2 - HALO + by * TY;
+  fence_proxy_async_smem();
+  mbar_expect_tx(tt.bar, bytes);
+  tma_load_3d(T.S, tt.ms, x, y, 0, tt.bar);
+  tma_load_3d(BG ? static_cast<void*>(T.G) : static_cast<void*>(T.R), tt.mg, x, y, BG ? 0 : 1, tt.bar);
+}
+
+// The stage for tile (bx, by) of one grid; the single-run kernels below and
+// in stage2d_tma.cu and the batched kernel (batch.cu) call it.  TMA: the
+// state arrives by bulk tensor copy (tt: the block's copy schedule), and the
+// copy of the block's next tile is issued once this tile's staged arrays
+// are dead, so that it overlaps the stores.  Returns false when a copy did
+// not complete in time (FLAG_TMA_TIMEOUT set; the block must stop).
+template <int MODE, bool BG, bool MIX, bool O6 = false, bool CG = false, bool TMA = false>
+__device__ __forceinline__ bool stage2d_body(const KParams& P, const KBufs& B, int bx, int by,
+                                             const TmaTile* tt = nullptr) {
   using ST = typename Form<MIX>::S;
   extern __shared__ double smem[];
   T2<BG, MIX> T;
   unsigned char* sp = reinterpret_cast<unsigned char*>(smem);
+  // the copy boxes land on 128-byte boundaries (the launch adds the slack)
+  if constexpr (TMA) sp = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(sp) + 127) & ~uintptr_t(127));
   T.S = reinterpret_cast<ST*>(sp);
   sp += 6 * RC * sizeof(ST);
   T.G = reinterpret_cast<double*>(sp);
@@ -362,16 +386,48 @@ __device__ __forceinline__ void stage2d_body(const KParams& P, const KBufs& B, i
   T.rd1 = T.rd0 + RX;
   T.U = T.rd1 + RY;
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
-  T.x0 = 2 + bx * TX;
+  T.x0 = XORG + bx * TX;
   T.y0 = 2 + by * TY;
   const int n0 = P.n0, n1 = P.n1;
-  // region columns x0-3 .. x0+TX+2 (rows likewise) inside [0, n-1]: no
-  // bounds or pad checks in the staging, flux and cross-term loops
-  T.inner = bx >= 1 && by >= 1 && T.x0 + TX + HALO <= n0 && T.y0 + TY + HALO <= n1;
+  // region columns x0-3 .. x0-3+RX-1 (rows y0-3 .. y0+TY+2) inside
+  // [0, n-1]: no bounds or pad checks in the staging, flux and cross-term
+  // loops
+  T.inner = bx >= 1 && by >= 1 && T.x0 - HALO + RX <= n0 && T.y0 + TY + HALO <= n1;
   const long nc = P.ncell;
   const ST* uin = static_cast<const ST*>(B.uin);
 
   // ---- stage the tile, 1/rho_t, the metric -------------------------------
+  if constexpr (TMA) {
+    if (tt->issue_self && tid == 0) tma_stage_issue(T, *tt, bx, by);
+    const bool ok = mbar_wait(tt->bar, tt->parity, TMA_WAIT_NS);
+    if (__syncthreads_or(!ok)) {
+      if (tid == 0) {
+        atomicOr(B.flags, FLAG_TMA_TIMEOUT);
+        mbar_wait(tt->bar, tt->parity, TMA_WAIT_NS);  // the copy in flight
+      }
+      __syncthreads();
+      return false;
+    }
+    for (int r = tid; r < RC; r += NTHREADS) {
+      const int lx = r % RX, ly = r / RX;
+      const int gi = T.x0 - HALO + lx, gj = T.y0 - HALO + ly;
+      const bool in = T.inner || (gi >= 0 && gi < n0 && gj >= 0 && gj < n1);
+      const double rho = (double)T.S[r];  // 0 outside the grid (the copy's fill)
+      double rhob;
+      if (BG) {
+        if (!in) T.G[1 * RC + r] = 1.0;
+        rhob = T.G[1 * RC + r];
+      } else {
+        rhob = in ? T.R[r] : 1.0;
+      }
+      const double rinv = 1.0 / (rho + rhob);
+      T.R[r] = rinv;
+      if (BG) {
+        T.V[r] = (double)T.S[M1 * RC + r] * rinv;
+        T.V[RC + r] = (double)T.S[M2 * RC + r] * rinv;
+      }
+    }
+  } else {
   for (int r = tid; r < RC; r += NTHREADS) {
     const int lx = r % RX, ly = r / RX;
     const int gi = T.x0 - HALO + lx, gj = T.y0 - HALO + ly;
@@ -401,6 +457,7 @@ __device__ __forceinline__ void stage2d_body(const KParams& P, const KBufs& B, i
       T.V[r] = (double)T.S[M1 * RC + r] * rinv;
       T.V[RC + r] = (double)T.S[M2 * RC + r] * rinv;
     }
+  }
   }
   for (int r = tid; r < RX + RY; r += NTHREADS) {
     if (r < RX) {
@@ -437,7 +494,7 @@ __device__ __forceinline__ void stage2d_body(const KParams& P, const KBufs& B, i
 
   const int lxo = tx + HALO, lyo = ty + HALO, lo = lyo * RX + lxo;
   const int gi = T.x0 + tx, gj = T.y0 + ty;
-  const bool active = gi <= n0 - 3 && gj <= n1 - 3;
+  const bool active = (XORG >= 2 || gi >= 2) && gi <= n0 - 3 && gj <= n1 - 3;
   const long co = active ? (long)gj * n0 + gi : 0;
 
   double out[6];
@@ -550,9 +607,10 @@ __device__ __forceinline__ void stage2d_body(const KParams& P, const KBufs& B, i
 
   // ---- combine, write, ghost images, CFL maxima -----------------------------
   double cm0 = P.cmax_floor[0], cm1 = P.cmax_floor[1];
+  double res[6] = {0, 0, 0, 0, 0, 0};
+  const bool is_base = (MODE == SMAUG_INT_EULER) || B.stage == 3;
+  double gb[4] = {0, 0, 0, 0};  // background fields at the tile cell
   if (active) {
-    double res[6];
-    const bool is_base = (MODE == SMAUG_INT_EULER) || B.stage == 3;
     if (MODE == SMAUG_INT_EULER) {
 #pragma unroll
       for (int f = 0; f < 6; f++) res[f] = out[f];
@@ -578,6 +636,19 @@ __device__ __forceinline__ void stage2d_body(const KParams& P, const KBufs& B, i
 #pragma unroll
     for (int f = 0; f < 6; f++) bad |= !isfinite(res[f]);
     if (bad) atomicOr(B.flags, 1);
+    if (BG) {
+      gb[0] = T.v(EB, lo);
+      gb[1] = T.v(RHOB, lo);
+      gb[2] = T.v(BB1, lo);
+      gb[3] = T.v(BB2, lo);
+    }
+  }
+  if constexpr (TMA) {
+    // the staged state is dead: copy the block's next tile during the stores
+    __syncthreads();
+    if (tid == 0 && tt->nbx >= 0) tma_stage_issue(T, *tt, tt->nbx, tt->nby);
+  }
+  if (active) {
     int ix[3], iy[3];
     ix[0] = gi;
     iy[0] = gj;
@@ -599,7 +670,7 @@ __device__ __forceinline__ void stage2d_body(const KParams& P, const KBufs& B, i
         for (int f = 0; f < 6; f++) store_value<MIX>(B, f * nc + cc, r[f], is_base);
         double eb, rb, b1b, b2b;
         if (BG && a2 == 0 && b == 0) {
-          eb = T.v(EB, lo); rb = T.v(RHOB, lo); b1b = T.v(BB1, lo); b2b = T.v(BB2, lo);
+          eb = gb[0]; rb = gb[1]; b1b = gb[2]; b2b = gb[3];
         } else {
           eb = B.bg[0 * nc + cc]; rb = B.bg[1 * nc + cc]; b1b = B.bg[2 * nc + cc]; b2b = B.bg[3 * nc + cc];
         }
@@ -624,6 +695,7 @@ __device__ __forceinline__ void stage2d_body(const KParams& P, const KBufs& B, i
     for (int w = 0; w < NTHREADS / 32; w++) v = dmax0(v, red[w][tid]);
     atomicMax(&B.cmax_out[tid], (unsigned long long)__double_as_longlong(v));
   }
+  return true;
 }
 
 template <int MODE, bool BG, bool MIX, bool O6>

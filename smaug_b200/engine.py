@@ -27,7 +27,7 @@ EXPORTS = [
     "smaug_adj_tape_reserve", "smaug_adj_forward_tape", "smaug_adj_backward_tape",
     "smaug_adj_destroy", "smaug_write_out_async", "smaug_wait_writes",
     "smaug_adj_backward_tape_range", "smaug_batch_tile_shape", "smaug_batch_pin_tile_shape",
-    "smaug_batch_persistent", "smaug_batch_pin_form",
+    "smaug_batch_persistent", "smaug_batch_pin_form", "smaug_staging", "smaug_set_staging",
 ]
 
 ERRORS = {1: "invalid", 2: "cuda", 3: "nomem", 4: "io", 5: "format", 6: "unsupported",
@@ -65,6 +65,8 @@ def lib():
         L.smaug_set_state.argtypes = [vp, dp]
         L.smaug_get_time.argtypes = [vp, ctypes.POINTER(ctypes.c_int64), dp, dp]
         L.smaug_get_cmax.argtypes = [vp, dp]
+        L.smaug_staging.argtypes = [vp, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32)]
+        L.smaug_set_staging.argtypes = [vp, ctypes.c_int32]
         L.smaug_write_out.argtypes = [vp, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int32,
                                       ctypes.c_double]
         L.smaug_write_out_async.argtypes = [vp, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int32,
@@ -215,6 +217,20 @@ class Engine:
         c = np.zeros(3)
         _check(lib().smaug_get_cmax(self.h, _dp(c)))
         return c[: self.p.ndim]
+
+    def staging(self):
+        """(tma, available): how the 2D stage tiles are staged (0 per-thread
+        loads, 1 bulk tensor copies in a persistent grid, 2 bulk tensor
+        copies with a block per tile), and whether the grid admits copies."""
+        on, av = ctypes.c_int32(0), ctypes.c_int32(0)
+        _check(lib().smaug_staging(self.h, ctypes.byref(on), ctypes.byref(av)))
+        return int(on.value), bool(av.value)
+
+    def set_staging(self, tma):
+        """Staging of the 2D tiles from the next launch on (0 / False
+        per-thread loads, 1 / True bulk tensor copies in a persistent grid, 2
+        bulk tensor copies with a block per tile); bitwise-identical results."""
+        _check(lib().smaug_set_staging(self.h, int(tma)))
 
     def write_out(self, path, name="test1", it=None, t=None):
         i, tt, _ = self.time()
