@@ -783,6 +783,9 @@ def main():
     ap.add_argument("--ref-sample", type=int, default=512)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ref-gpu", action="store_true")
+    ap.add_argument("--staging", type=int, default=0, choices=[0, 1, 2],
+                    help="2D tile staging: 0 per-thread loads (default), 1 bulk tensor copies in a "
+                         "persistent grid, 2 bulk tensor copies with a block per tile")
     ap.add_argument("--no-mixed", dest="mixed", action="store_false",
                     help="skip the mixed precision measurement")
     args = ap.parse_args()
@@ -825,6 +828,8 @@ def main():
     stream = torch.cuda.Stream()
     assert stream.cuda_stream != 0
     eng.set_stream(stream.cuda_stream)
+    if args.staging:
+        eng.set_staging(args.staging)
     alg_bytes = alg_bytes_per_cell_step(p.ndim)
 
     def barrier():
@@ -874,6 +879,25 @@ def main():
     e2e_val = ncell_int * args.e2e_steps * ws / (e2e_ms / 1e3) / 1e6
     h2d = (2 + 2 * p.ndim) * p.ncells * 8
     d2h = nevo * p.ncells * 8
+    # the other tile stagings of the 2D kernel on the same engine (bitwise the
+    # same arithmetic), timed like the headline
+    staging = None
+    if p.ndim == 2 and eng.staging()[1]:
+        staging = {"selected": args.staging, "ms_per_step": {}}
+        names = {0: "per-thread loads", 1: "bulk tensor copies, persistent grid",
+                 2: "bulk tensor copies, a block per tile"}
+        for mode in (0, 1, 2):
+            eng.set_staging(mode)
+            eng.step_async(args.warmup)
+            s0 = torch.cuda.Event(enable_timing=True)
+            s1 = torch.cuda.Event(enable_timing=True)
+            s0.record(stream)
+            eng.step_async(args.steps)
+            s1.record(stream)
+            torch.cuda.synchronize()
+            eng.sync()
+            staging["ms_per_step"][names[mode]] = max_over_ranks(s0.elapsed_time(s1), ws) / args.steps
+        eng.set_staging(args.staging)
     eng.close()
 
     # the mixed precision form on the same workload: same warm-up and timed
@@ -885,6 +909,8 @@ def main():
         pm.precision = P.PREC_MIXED
         em = engine.Engine(pm, w, pos)
         em.set_stream(stream.cuda_stream)
+        if args.staging and em.staging()[1]:
+            em.set_staging(args.staging)
         em.step_async(args.warmup)
         em.sync()
         torch.cuda.synchronize()
@@ -942,6 +968,7 @@ def main():
             "fp64_roofline": fp64_roofline(p.ndim, args.precision, ncell_int, args.steps, ms_max),
             "clocks": clk.summary(),
             "mixed": mixed,
+            "staging": staging,
         }
         if ws == 1 and not args.no_cpu_baseline and args.workload == "ot":
             os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))

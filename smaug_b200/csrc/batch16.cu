@@ -9,6 +9,7 @@ namespace t16x16 {
 constexpr int TX = 16, TY = 16;
 constexpr int RX = TX + 2 * HALO, RY = TY + 2 * HALO;
 constexpr int RC = RX * RY;
+constexpr int RXU = RX;
 constexpr int NTHREADS = TX * TY;
 
 #include "stage2d.cuh"

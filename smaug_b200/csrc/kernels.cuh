@@ -31,6 +31,7 @@ constexpr int HALO = 3;            // stencil radius of the hyperdiffusion windo
 constexpr int RX = TX + 2 * HALO;  // staged region
 constexpr int RY = TY + 2 * HALO;
 constexpr int RC = RX * RY;
+constexpr int RXU = RX;            // columns of a region row that the stage reads
 constexpr int NTHREADS = TX * TY;
 constexpr int XORG = 2;            // x index of the first cell of tile column 0
 

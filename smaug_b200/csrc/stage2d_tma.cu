@@ -35,6 +35,7 @@ constexpr int TX = 32, TY = 8;
 constexpr int RX = TX + 8;  // 3 + 32 + 5 columns: 16-byte-multiple rows in float and double
 constexpr int RY = TY + 2 * HALO;
 constexpr int RC = RX * RY;
+constexpr int RXU = TX + 2 * HALO;  // the last two columns of a row are copied, never read
 constexpr int NTHREADS = TX * TY;
 constexpr int XORG = 3 - TX;  // tile column bx starts at 3 + TX (bx - 1)
 static_assert((XORG - HALO) % 32 == 0, "region start must be a multiple of 32 cells");
