@@ -149,6 +149,9 @@ __device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
                : "memory");
 }
+__device__ __forceinline__ void mbar_arrive(unsigned long long* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
 // box of a 3D tensor map ([z][y][x], x fastest) at (x, y, z) into shared
 // memory; x * element size must be a multiple of 16 bytes
 __device__ __forceinline__ void tma_load_3d(void* dst, const void* map, int x, int y, int z,
@@ -160,16 +163,19 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const void* map, int x, i
       : "memory");
 }
 // Wait until the barrier's phase of parity `parity` has completed; false
-// when it has not after limit_ns nanoseconds of the global timer.
+// when it has not after limit_ns nanoseconds of the global timer.  Each try
+// may suspend the thread for up to TRY_WAIT_HINT_NS instead of returning at
+// once, so waiting warps do not spin on the shared-memory pipe.
+constexpr unsigned TRY_WAIT_HINT_NS = 20000;
 __device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity, unsigned long long limit_ns) {
   const unsigned a = smem_u32(bar);
   unsigned long long t0 = 0;
   for (unsigned i = 0;; i++) {
     unsigned done;
     asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}"
         : "=r"(done)
-        : "r"(a), "r"(parity)
+        : "r"(a), "r"(parity), "r"(TRY_WAIT_HINT_NS)
         : "memory");
     if (done) return true;
     if ((i & 63) == 0) {

@@ -346,39 +346,52 @@ __device__ __forceinline__ void hyper_pass(const T2<BG, MIX>& T, const KParams& 
 }
 
 // Bulk tensor copy of the staged state of tile (bx, by) -- the 6 fields in
-// the storage type into T.S, and the 4 background fields into T.G (with
-// background fields) or rho_b alone into T.R (without) -- completing on
-// tt.bar.  Cells outside the grid read 0.  The region starts at column
+// the storage type into s, and (gdst non-null) the 4 background fields
+// (with background fields) or rho_b alone (without) into gdst -- completing
+// on tt.bar.  Cells outside the grid read 0.  The region starts at column
 // x0 - HALO = XORG - HALO + bx TX, which the TMA-staged kernel's tile origin
 // makes a multiple of 32 cells (the copy's x offset must be 16-byte aligned).
 template <bool BG, bool MIX>
-__device__ __forceinline__ void tma_stage_issue(const T2<BG, MIX>& T, const TmaTile& tt, int bx, int by) {
+__device__ __forceinline__ void tma_stage_issue(void* s, void* gdst, const TmaTile& tt, int bx, int by) {
   using ST = typename Form<MIX>::S;
-  constexpr unsigned bytes = 6 * RC * sizeof(ST) + (BG ? 4 : 1) * RC * sizeof(double);
+  const unsigned bytes = (s ? 6 * RC * sizeof(ST) : 0) + (gdst ? (BG ? 4 : 1) * RC * sizeof(double) : 0);
   const int x = XORG - HALO + bx * TX, y = 2 - HALO + by * TY;
   fence_proxy_async_smem();
   mbar_expect_tx(tt.bar, bytes);
-  tma_load_3d(T.S, tt.ms, x, y, 0, tt.bar);
-  tma_load_3d(BG ? static_cast<void*>(T.G) : static_cast<void*>(T.R), tt.mg, x, y, BG ? 0 : 1, tt.bar);
+  if (s) tma_load_3d(s, tt.ms, x, y, 0, tt.bar);
+  if (gdst) tma_load_3d(gdst, tt.mg, x, y, BG ? 0 : 1, tt.bar);
 }
 
 // The stage for tile (bx, by) of one grid; the single-run kernels below and
-// in stage2d_tma.cu and the batched kernel (batch.cu) call it.  TMA: the
+// in stage2d_tma.cu and the batched kernel (batch.cu) call it.  TMA = 1: the
 // state arrives by bulk tensor copy (tt: the block's copy schedule), and the
 // copy of the block's next tile is issued once this tile's staged arrays
-// are dead, so that it overlaps the stores.  Returns false when a copy did
+// are dead, so that it overlaps the stores.  TMA = 2 (no background
+// fields): two state buffers; the copy of the next tile's state goes to the
+// other buffer as soon as this tile's copy has arrived, so that it overlaps
+// the whole tile, and its rho_b (into 1/rho_t's array, dead by then) during
+// the stores -- two arrivals on the barrier per phase.  Returns false when a copy did
 // not complete in time (FLAG_TMA_TIMEOUT set; the block must stop).
-template <int MODE, bool BG, bool MIX, bool O6 = false, bool CG = false, bool TMA = false>
+template <int MODE, bool BG, bool MIX, bool O6 = false, bool CG = false, int TMA = 0>
 __device__ __forceinline__ bool stage2d_body(const KParams& P, const KBufs& B, int bx, int by,
                                              const TmaTile* tt = nullptr) {
   using ST = typename Form<MIX>::S;
   extern __shared__ double smem[];
   T2<BG, MIX> T;
   unsigned char* sp = reinterpret_cast<unsigned char*>(smem);
-  // the copy boxes land on 128-byte boundaries (the launch adds the slack)
-  if constexpr (TMA) sp = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(sp) + 127) & ~uintptr_t(127));
+  // the copy boxes land on 128-byte boundaries (the launch adds the slack);
+  // an offset added to the shared array itself, so that the compiler still
+  // addresses the tile arrays as shared memory (a pointer rebuilt from an
+  // integer would make every tile access a generic one)
+  if constexpr (TMA != 0) sp += (128u - (smem_u32(sp) & 127u)) & 127u;
+  static_assert(TMA != 2 || !BG, "double-buffered staging without background fields only");
   T.S = reinterpret_cast<ST*>(sp);
   sp += 6 * RC * sizeof(ST);
+  ST* const s_other = reinterpret_cast<ST*>(sp);  // TMA = 2: the second state buffer
+  if constexpr (TMA == 2) {
+    if (tt->parity) T.S = s_other;
+    sp += 6 * RC * sizeof(ST);
+  }
   T.G = reinterpret_cast<double*>(sp);
   sp += (BG ? 4 * RC : 0) * sizeof(double);
   T.R = reinterpret_cast<double*>(sp);
@@ -403,7 +416,11 @@ __device__ __forceinline__ bool stage2d_body(const KParams& P, const KBufs& B, i
   if constexpr (TMA) {
     // every thread waits on the barrier (one waiter and a block barrier
     // measured 2.5 % slower at 4096^2)
-    if (tt->issue_self && tid == 0) tma_stage_issue(T, *tt, bx, by);
+    void* const gdst = BG ? static_cast<void*>(T.G) : static_cast<void*>(T.R);
+    if (tt->issue_self && tid == 0) {
+      tma_stage_issue<BG, MIX>(T.S, gdst, *tt, bx, by);
+      if (TMA == 2) mbar_arrive(tt->bar);  // the phase's second arrival
+    }
     const bool ok = mbar_wait(tt->bar, tt->parity, TMA_WAIT_NS);
     if (__syncthreads_or(!ok)) {
       if (tid == 0) {
@@ -412,6 +429,13 @@ __device__ __forceinline__ bool stage2d_body(const KParams& P, const KBufs& B, i
       }
       __syncthreads();
       return false;
+    }
+    if constexpr (TMA == 2) {
+      // the other buffer's last reader, the previous tile, is done
+      if (tid == 0 && tt->nbx >= 0) {
+        ST* const s0 = reinterpret_cast<ST*>(reinterpret_cast<unsigned char*>(s_other) - 6 * RC * sizeof(ST));
+        tma_stage_issue<BG, MIX>(tt->parity ? s0 : s_other, nullptr, *tt, tt->nbx, tt->nby);
+      }
     }
     for (int u = tid; u < RXU * RY; u += NTHREADS) {
       const int lx = u % RXU, ly = u / RXU, r = ly * RX + lx;
@@ -648,10 +672,13 @@ __device__ __forceinline__ bool stage2d_body(const KParams& P, const KBufs& B, i
       gb[3] = T.v(BB2, lo);
     }
   }
-  if constexpr (TMA) {
-    // the staged state is dead: copy the block's next tile during the stores
+  if constexpr (TMA != 0) {
+    // the staged arrays are dead: copy the block's next tile (TMA = 2: its
+    // rho_b) during the stores
     __syncthreads();
-    if (tid == 0 && tt->nbx >= 0) tma_stage_issue(T, *tt, tt->nbx, tt->nby);
+    if (tid == 0 && tt->nbx >= 0)
+      tma_stage_issue<BG, MIX>(TMA == 2 ? nullptr : static_cast<void*>(T.S),
+                               BG ? static_cast<void*>(T.G) : static_cast<void*>(T.R), *tt, tt->nbx, tt->nby);
   }
   if (active) {
     int ix[3], iy[3];

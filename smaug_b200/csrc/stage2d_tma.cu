@@ -35,7 +35,8 @@ constexpr int TX = 32, TY = 8;
 constexpr int RX = TX + 8;  // 3 + 32 + 5 columns: 16-byte-multiple rows in float and double
 constexpr int RY = TY + 2 * HALO;
 constexpr int RC = RX * RY;
-constexpr int RXU = TX + 2 * HALO;  // the last two columns of a row are copied, never read
+constexpr int RXU = RX;  // all 40 columns (the last two are never read; skipping them in the
+                        // region loops measured more shared-memory bank conflicts)
 constexpr int NTHREADS = TX * TY;
 constexpr int XORG = 3 - TX;  // tile column bx starts at 3 + TX (bx - 1)
 static_assert((XORG - HALO) % 32 == 0, "region start must be a multiple of 32 cells");
@@ -43,12 +44,21 @@ static_assert(RX * sizeof(float) % 16 == 0 && RX * sizeof(double) % 16 == 0, "ro
 
 #include "stage2d.cuh"
 
+// the staging of a specialisation: two state buffers where they keep 4
+// blocks per SM (the mixed form without background fields), else one
+template <bool BG, bool MIX>
+__host__ __device__ constexpr int tma_form() {
+  return (!BG && MIX) ? 2 : 1;
+}
+
 template <int MODE, bool BG, bool MIX>
 __global__ void __launch_bounds__(NTHREADS, SMAUG_MINB2D)
     stage2d_tma_kernel(const KParams P, const KBufs B, const __grid_constant__ CUtensorMap ms,
                        const __grid_constant__ CUtensorMap mg, int nbx, int ntiles) {
   __shared__ unsigned long long bar;
-  if (threadIdx.x == 0 && threadIdx.y == 0) mbar_init(&bar, 1);
+  // arrivals per phase: the copy of the state and, with two state buffers,
+  // the separate copy of rho_b
+  if (threadIdx.x == 0 && threadIdx.y == 0) mbar_init(&bar, tma_form<BG, MIX>());
   __syncthreads();
   TmaTile tt{&ms, &mg, &bar, 0u, true, -1, 0};
   unsigned k = 0;
@@ -58,7 +68,8 @@ __global__ void __launch_bounds__(NTHREADS, SMAUG_MINB2D)
     tt.issue_self = k == 0;
     tt.nbx = next < ntiles ? next % nbx : -1;
     tt.nby = next / nbx;
-    if (!stage2d_body<MODE, BG, MIX, false, false, true>(P, B, tile % nbx, tile / nbx, &tt)) return;
+    if (!stage2d_body<MODE, BG, MIX, false, false, tma_form<BG, MIX>()>(P, B, tile % nbx, tile / nbx, &tt))
+      return;
   }
 }
 
@@ -66,7 +77,8 @@ __global__ void __launch_bounds__(NTHREADS, SMAUG_MINB2D)
 // body rounds its base up to 128 bytes for the copies)
 template <bool BG, bool MIX>
 constexpr size_t tma_smem() {
-  return s2::smem_bytes<BG, MIX, false>() + 128;
+  return s2::smem_bytes<BG, MIX, false>() + 128 +
+         (tma_form<BG, MIX>() == 2 ? 6 * RC * sizeof(typename Form<MIX>::S) : 0);
 }
 
 template <int MODE, bool BG, bool MIX>
