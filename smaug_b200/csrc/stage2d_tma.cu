@@ -11,19 +11,24 @@
 //
 // One thread issues the copies of a tile -- the 6 fields of the stage input
 // as one box [6][14][40], and the 4 background fields (or rho_b alone) as a
-// second box -- completing on the block's mbarrier.  Two launch forms:
-// persistent (grid = resident blocks per SM x SMs; block b owns the tiles
-// b, b + grid, ... and issues the copy of its next tile as soon as the
-// current tile's staged arrays are dead, after its last hyperdiffusion pass
-// and the reads of its combine, so that the copy overlaps the tile's stores,
-// ghost images and CFL epilogue), or one block per tile.  Cells outside the
-// grid read 0 (the copy's fill value), as the per-thread staging stores
-// them.  Every wait on the mbarrier is bounded (TMA_WAIT_NS); a block whose
-// copy does not arrive sets FLAG_TMA_TIMEOUT, waits (bounded) for its copy
-// in flight and exits.
+// second box -- completing on the block's mbarrier.  Two launch forms: one
+// block per tile, or a persistent grid (resident blocks per SM x SMs; block
+// b owns the tiles b, b + grid, ...).  In the persistent form a block copies
+// its next tile as soon as the current tile's staged arrays are dead (after
+// the last hyperdiffusion pass and the reads of its combine), overlapping
+// the copy with the tile's stores, ghost images and CFL epilogue; the mixed
+// form without background fields, where a second state buffer still fits 4
+// blocks per SM, copies the next tile's state into the other buffer a whole
+// tile ahead and its rho_b during the stores (two arrivals per phase).
+// Cells outside the grid read 0 (the copy's fill value), as the per-thread
+// staging stores them.  Every wait on the mbarrier is bounded (TMA_WAIT_NS);
+// a block whose copy does not arrive sets FLAG_TMA_TIMEOUT, waits (bounded)
+// for its copies in flight and exits.
 //
 // The arithmetic is the per-thread-staged kernel's, cell for cell, so the
-// kernels' results are bitwise identical.
+// kernels' results are bitwise identical.  On B200 at 4096^2 these kernels
+// run about 10 % slower than the per-thread staging (RK4 FP64 11.4 vs 10.5 ms
+// per step, mixed 10.5 vs 9.5), which therefore stays the engine's default.
 #include <cuda.h>
 
 #include "kernels.cuh"
