@@ -110,20 +110,19 @@ using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, 
                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 
+// the driver's tensor-map encoder, looked up once (a function-local static
+// is initialised once even when engines are created from several threads)
 static EncodeTiled encode_tiled() {
-  static EncodeTiled fn = nullptr;
-  static bool tried = false;
-  if (!tried) {
-    tried = true;
+  static const EncodeTiled fn = [] {
     void* p = nullptr;
     cudaDriverEntryPointQueryResult q;
     if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) ==
             cudaSuccess &&
         q == cudaDriverEntryPointSuccess)
-      fn = reinterpret_cast<EncodeTiled>(p);
-    else
-      cudaGetLastError();
-  }
+      return reinterpret_cast<EncodeTiled>(p);
+    cudaGetLastError();
+    return static_cast<EncodeTiled>(nullptr);
+  }();
   return fn;
 }
 
